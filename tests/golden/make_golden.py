@@ -1,0 +1,396 @@
+"""Generate golden input/output vectors from the unmodified PyTICC reference.
+
+Run once in a container that has the reference checked out (JAX itself is not
+needed: ``tests/golden/_jaxshim`` is a NumPy-backed stand-in for the few JAX calls
+the reference makes)::
+
+    python tests/golden/make_golden.py /path/to/PyTICC/src
+
+Every fixture is a small ``.npz`` written next to this script.  The product never
+reads these files; ``tests/`` uses them to pin the oracle and the CUDA path.
+
+Synthetic systems follow the shapes of the benchmark configurations at reduced
+sizes (fewer rotor states, shorter radial grids, fewer energies) so that the
+reference finishes in seconds.  The parameters are stored in each fixture's
+``params_json`` entry and are mirrored by ``pyticc_b200.workloads``.
+"""
+
+from __future__ import annotations
+
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE / "_jaxshim"))
+sys.path.insert(1, sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+
+from loguru import logger  # noqa: E402
+
+logger.remove()
+
+import pyticc as ticc  # noqa: E402
+from pyticc.basis.angle import gauss_legendre_dvr  # noqa: E402
+from pyticc.basis.dvr import build_RovibDVR, build_SineDVR  # noqa: E402
+from pyticc.basis.rovib import RovibBasis  # noqa: E402
+from pyticc.match import bessel as ref_bessel  # noqa: E402
+from pyticc.match import get_Smat  # noqa: E402
+from pyticc.matrix.interaction.common import VBasisBF, contract  # noqa: E402
+from pyticc.propagation.grid import build_radial_sectors, iter_radial_windows  # noqa: E402
+from pyticc.propagation.logd import propagate_logD  # noqa: E402
+
+CM = ticc.CM2AU
+AMU = 1822.888486209
+K2AU = 1.0 / 315775.02480407
+
+
+def _save(name: str, params: dict, **arrays) -> None:
+    payload = {key: np.asarray(value) for key, value in arrays.items()}
+    payload["params_json"] = np.asarray(json.dumps(params))
+    np.savez_compressed(HERE / f"{name}.npz", **payload)
+    size = (HERE / f"{name}.npz").stat().st_size
+    print(f"wrote {name}.npz ({size / 1024:.1f} KiB)")
+
+
+def _legendre(n: int, x: np.ndarray) -> np.ndarray:
+    from numpy.polynomial import legendre
+
+    coefficients = np.zeros(n + 1)
+    coefficients[n] = 1.0
+    return legendre.legval(x, coefficients)
+
+
+# ----------------------------------------------------------------------------------------
+# Unit-level fixtures
+# ----------------------------------------------------------------------------------------
+def make_ldmd() -> None:
+    rng = np.random.default_rng(1234)
+    for mode, n_channel in (("real", 6), ("capture", 5)):
+        n_sector, n_energy = 9, 3
+        reduced_mass = 1.7
+        half_steps = rng.uniform(0.03, 0.08, size=n_sector)
+        base = rng.normal(size=(n_channel, n_channel)) * 0.4
+        base = 0.5 * (base + base.T) + np.diag(rng.uniform(-2.0, 6.0, size=n_channel))
+        W = []
+        for point in range(2 * n_sector + 1):
+            drift = rng.normal(size=(n_channel, n_channel)) * 0.05
+            W.append(base + 0.5 * (drift + drift.T) + 0.02 * point * np.eye(n_channel))
+        W = np.asarray(W)
+        energies = rng.uniform(0.05, 0.9, size=n_energy)
+        W0 = W[0][None] - 2.0 * reduced_mass * energies[:, None, None] * np.eye(n_channel)
+        if mode == "real":
+            Y0 = np.asarray(ticc.propagation.initialize_logD_inelastic(W0))
+        else:
+            Y0 = np.asarray(ticc.propagation.initialize_logD_capture(W0))
+        Y = np.asarray(propagate_logD(Y0, energies, reduced_mass, half_steps, W[0:-1:2], W[1::2], W[2::2]))
+        _save(
+            f"ldmd_{mode}",
+            {"mode": mode, "reduced_mass": reduced_mass},
+            Y_initial=Y0,
+            energies=energies,
+            half_steps=half_steps,
+            W_points=W,
+            Y_final=Y,
+        )
+
+
+def make_contract() -> None:
+    rng = np.random.default_rng(77)
+    grid_shape = (3, 5)
+    n_grid = 15
+    groups = {0: (0, 3, 4), 1: (1, 5), 2: (2, 6, 7, 8)}
+    n_channel = 9
+    B_real = {K: rng.normal(size=(len(idx), n_grid)) for K, idx in groups.items()}
+    B_imag = {K: rng.normal(size=(len(idx), n_grid)) for K, idx in groups.items()}
+    potential = rng.normal(size=(4, *grid_shape))
+    out = {}
+    for tag, imag, norm in (("real", None, 1.0), ("complex", B_imag, 0.3)):
+        basis = VBasisBF(n_channel=n_channel, grid_shape=grid_shape, channel_indices=groups, B_real=B_real, B_imag=imag, normalization=norm)
+        out[f"V_{tag}"] = contract(basis, potential)
+        out[f"V_{tag}_subset"] = contract(basis, potential, (7, 0, 5, 2))
+    _save(
+        "contract",
+        {"groups": {str(K): list(v) for K, v in groups.items()}, "n_channel": n_channel, "grid_shape": list(grid_shape), "norm_complex": 0.3},
+        potential=potential,
+        **{f"B_real_{K}": v for K, v in B_real.items()},
+        **{f"B_imag_{K}": v for K, v in B_imag.items()},
+        **out,
+    )
+
+
+def make_smatrix() -> None:
+    rng = np.random.default_rng(5)
+    n_channel = 6
+    E_int = np.array([0.0, 0.05, 0.11, 0.3, 0.45, 0.8])
+    L = np.array([0.0, 1.0, 2.35, 1.7, 4.2, 6.0])
+    energies = np.array([0.2, 0.5, 0.07])
+    reduced_mass = 2.5
+    Rmatch = 9.0
+    real = []
+    for _ in energies:
+        M = rng.normal(size=(n_channel, n_channel)) * 0.3
+        real.append(0.5 * (M + M.T) + np.diag(rng.uniform(-1.5, 1.0, size=n_channel)))
+    real = np.asarray(real)
+    S_real = get_Smat(real, Rmatch, energies, reduced_mass, E_int, L)
+    imag = np.asarray([-0.2 * np.diag(rng.uniform(0.1, 1.0, size=n_channel)) for _ in energies])
+    S_complex = get_Smat(real + 1j * imag, Rmatch, energies, reduced_mass, E_int, L)
+
+    def pad(mats):
+        outp = np.zeros((len(mats), n_channel, n_channel), dtype=np.complex128)
+        for i, m in enumerate(mats):
+            outp[i, : m.shape[0], : m.shape[1]] = m
+        return outp
+
+    _save(
+        "smatrix",
+        {"reduced_mass": reduced_mass, "Rmatch": Rmatch},
+        E_int=E_int,
+        L=L,
+        energies=energies,
+        Y_real=real,
+        Y_complex=real + 1j * imag,
+        S_real=pad(S_real),
+        S_complex=pad(S_complex),
+        n_open=np.array([m.shape[0] for m in S_real]),
+    )
+
+
+def make_bessel() -> None:
+    ells = np.array([0.0, 0.3, 1.0, 2.7, 10.0, 25.5, 60.0, 3.0000000000001])
+    xs = np.array([0.01, 0.5, 1.9, 2.1, 5.0, 20.0, 100.0, 500.0, 1500.0])
+    rows = []
+    for ell in ells:
+        for x in xs:
+            try:
+                values = ref_bessel.riccati_bessel_jy(float(ell), float(x))
+            except ValueError:
+                continue
+            rows.append([ell, x, *values])
+    nus = np.array([0.5, 0.8, 1.5, 3.2, 10.5, 30.5, 60.5])
+    krows = []
+    for nu in nus:
+        for x in np.array([0.01, 0.5, 1.9, 2.1, 5.0, 40.0, 300.0, 2500.0]):
+            try:
+                krows.append([nu, x, ref_bessel.modified_bessel_K_logD(float(nu), float(x))])
+            except ValueError:
+                continue
+    _save("bessel", {}, riccati=np.asarray(rows), k_logd=np.asarray(krows))
+
+
+def make_grid() -> None:
+    cases = [((2.5, 30.0), (0.05,)), ((2.5, 40.0), (0.02,)), ((3.0, 3.37, 5.0), (0.1, 0.07)), ((1.0, 1.05), (0.1,))]
+    payload = {}
+    for index, (boundaries, halves) in enumerate(cases):
+        sectors = build_radial_sectors(boundaries, halves)
+        payload[f"sectors_{index}"] = np.asarray([[s.radial_start, s.radial_end] for s in sectors])
+        windows = list(iter_radial_windows(sectors, n_grid=24, n_channel=231, n_energy=16, memory_limit_mb=64.0))
+        payload[f"window_sizes_{index}"] = np.asarray([len(w) for w, _ in windows])
+        payload[f"window_points_{index}"] = np.concatenate([p for _, p in windows])
+    _save("grid", {"cases": [[list(b), list(h)] for b, h in cases]}, **payload)
+
+
+# ----------------------------------------------------------------------------------------
+# End-to-end fixtures through ticc.prepare_potential / ticc.solve
+# ----------------------------------------------------------------------------------------
+def _rigid_rotor(B_cm: float, jmax: int) -> ticc.DiatomBasis:
+    energies = B_cm * CM * np.arange(jmax + 1) * (np.arange(jmax + 1) + 1.0)
+    rovib = RovibBasis(grids=np.array([1.5]), E_vj=energies[None, :], WF_vj=np.ones((1, 1, jmax + 1)))
+    return ticc.DiatomBasis(rovib=rovib, energy_zero=0.0)
+
+
+def _lj_aniso_pes(eps_cm: float, Rm: float, a1: float, a2: float, c1: float = 0.0, c2: float = 0.0, re: float = 1.4):
+    def interaction(R, coordinates):
+        r, theta = coordinates
+        x = np.cos(theta)
+        radial = eps_cm * CM * ((Rm / R) ** 12 - 2.0 * (Rm / R) ** 6)
+        aniso = 1.0 + a1 * (1.0 + c1 * (r - re)) * x + a2 * (1.0 + c2 * (r - re)) * 0.5 * (3.0 * x * x - 1.0)
+        return radial * aniso
+
+    return ticc.PESWrapper(interaction=interaction)
+
+
+def _pad_smat(smats, n_channel):
+    out = np.zeros((len(smats), n_channel, n_channel), dtype=np.complex128)
+    for i, m in enumerate(smats):
+        out[i, : m.shape[0], : m.shape[1]] = m
+    return out
+
+
+def _solve_and_save(name, params, system, boundaries, halves, energies, mode, memory_mb, **quad):
+    grid = ticc.prepare_potential(system, boundaries, halves, **quad)
+    result = ticc.solve(system, energies, grid, ticc.Propagation(mode=mode, memory_mb=memory_mb, device="cpu"))
+    basis = system.basis
+    channels = np.asarray([[c.mis_X.j, -1 if c.mis_X.v is None else c.mis_X.v, c.mis_Y.j, -1 if c.mis_Y.v is None else c.mis_Y.v, c.j_couple, c.K] for c in basis])
+    _save(
+        name,
+        params,
+        energies=np.asarray(energies),
+        E_int=basis.E_int,
+        channels=channels,
+        radial_points=grid.radial_points,
+        potential_values=np.asarray(grid.values),
+        U=ticc.scattering.ScattHamiltonian(basis=basis, reduced_mass=system.reduced_mass, interaction=lambda R: None).U,
+        Bmat=result.asymptotic_transform,
+        L=result.L,
+        Y_propagated=np.asarray(result.Y_propagated),
+        Smat=_pad_smat(result.Smat, basis.n_channel),
+        n_open=np.asarray([m.shape[0] for m in result.Smat]),
+        cos_theta=grid.coordinate("cos_theta") if grid.scattering_type is ticc.ScatteringType.ATOM_DIATOM else np.zeros(0),
+    )
+
+
+def make_solve_rigid() -> None:
+    params = {"B_cm": 20.0, "jmax": 5, "J": 3, "mu_amu": 18.0, "eps_cm": 150.0, "Rm": 6.5, "a1": 0.3, "a2": 0.2, "n_theta": 8, "boundaries": [2.5, 10.0], "half_steps": [0.05]}
+    energies = np.linspace(10.0, 500.0, 5) * CM
+    for parity in (1, -1):
+        system = ticc.build_ScattSystem(
+            ticc.AtomSpec(),
+            _rigid_rotor(params["B_cm"], params["jmax"]),
+            Jtot=params["J"],
+            system_parity=parity,
+            potential=_lj_aniso_pes(params["eps_cm"], params["Rm"], params["a1"], params["a2"]),
+            reduced_mass=params["mu_amu"] * AMU,
+        )
+        _solve_and_save(f"solve_rigid_p{'+' if parity > 0 else '-'}", {**params, "parity": parity}, system, params["boundaries"], params["half_steps"], energies, "inelastic", 512.0, n_theta=params["n_theta"])
+    # the same system in capture mode, with a memory budget small enough to force several windows
+    system = ticc.build_ScattSystem(
+        ticc.AtomSpec(),
+        _rigid_rotor(params["B_cm"], params["jmax"]),
+        Jtot=params["J"],
+        system_parity=1,
+        potential=_lj_aniso_pes(params["eps_cm"], params["Rm"], params["a1"], params["a2"]),
+        reduced_mass=params["mu_amu"] * AMU,
+    )
+    _solve_and_save("solve_rigid_capture", {**params, "parity": 1, "memory_mb": 0.05}, system, params["boundaries"], params["half_steps"], energies, "capture", 0.05, n_theta=params["n_theta"])
+
+
+def make_solve_morse() -> None:
+    params = {
+        "De_cm": 40000.0,
+        "re": 1.4,
+        "a": 1.2,
+        "diatom_mass_amu": 1.0,
+        "r_interval": [0.5, 3.5],
+        "n_dvr": 16,
+        "vmax": 1,
+        "jmax": 4,
+        "J": 2,
+        "mu_amu": 18.0,
+        "eps_cm": 150.0,
+        "Rm": 6.5,
+        "a1": 0.3,
+        "a2": 0.2,
+        "seed": 2024,
+        "n_theta": 6,
+        "boundaries": [2.5, 8.0],
+        "half_steps": [0.05],
+    }
+    c1, c2 = np.random.default_rng(params["seed"]).uniform(-0.5, 0.5, size=2)
+    params["c1"], params["c2"] = float(c1), float(c2)
+    mass = params["diatom_mass_amu"] * AMU
+
+    def morse(r):
+        return params["De_cm"] * CM * (1.0 - np.exp(-params["a"] * (r - params["re"]))) ** 2
+
+    dvr = build_SineDVR(params["r_interval"][0], params["r_interval"][1], params["n_dvr"], mass, morse)
+    rovib = build_RovibDVR(dvr, params["vmax"], params["jmax"], mass)
+    diatom = ticc.DiatomBasis(rovib=rovib, energy_zero=float(rovib.E_vj[0, 0]))
+    energies = np.array([100.0, 1100.0, 2500.0, 3000.0]) * CM
+    system = ticc.build_ScattSystem(
+        ticc.AtomSpec(),
+        diatom,
+        Jtot=params["J"],
+        system_parity=1,
+        potential=_lj_aniso_pes(params["eps_cm"], params["Rm"], params["a1"], params["a2"], c1, c2, params["re"]),
+        reduced_mass=params["mu_amu"] * AMU,
+    )
+    _solve_and_save("solve_morse", params, system, params["boundaries"], params["half_steps"], energies, "inelastic", 512.0, n_theta=params["n_theta"])
+    np.savez_compressed(HERE / "morse_rovib.npz", grids=rovib.grids, E_vj=rovib.E_vj, WF_vj=rovib.WF_vj)
+
+
+def make_solve_diatom_diatom() -> None:
+    params = {"B1_cm": 60.0, "B2_cm": 2.0, "jmax": 2, "J": 1, "mu_amu": 3.6, "lmax": 2, "seed": 11, "strength_cm": 40.0, "lj_eps_cm": 100.0, "lj_Rm": 6.0, "n_theta_X": 6, "n_theta_Y": 6, "n_phi": 5, "boundaries": [4.0, 10.0], "half_steps": [0.05]}
+    from pyticc.basis.angle import clebsch_gordan, norm_YjK
+
+    rng = np.random.default_rng(params["seed"])
+    terms = []
+    for l1 in range(params["lmax"] + 1):
+        for l2 in range(params["lmax"] + 1):
+            for lam in range(abs(l1 - l2), min(l1 + l2, params["lmax"]) + 1):
+                if (l1 + l2 + lam) % 2 == 0 and (l1, l2, lam) != (0, 0, 0):
+                    terms.append((l1, l2, lam, float(rng.normal())))
+
+    def interaction(R, coordinates):
+        _, _, t1, t2, phi = coordinates
+        x1, x2 = np.cos(t1), np.cos(t2)
+        total = np.zeros_like(x1)
+        for l1, l2, lam, c in terms:
+            angular = np.zeros_like(x1)
+            for m in range(-min(l1, l2), min(l1, l2) + 1):
+                angular += float(clebsch_gordan(l1, m, l2, -m, lam)) * norm_YjK(l1, m, x1) * norm_YjK(l2, -m, x2) * np.cos(m * phi)
+            total += c * angular
+        radial = params["strength_cm"] * CM * np.exp(-0.8 * (R - 6.0))
+        lj = params["lj_eps_cm"] * CM * ((params["lj_Rm"] / R) ** 12 - 2.0 * (params["lj_Rm"] / R) ** 6)
+        return radial * total + lj
+
+    params["terms"] = terms
+    diatom_X = _rigid_rotor(params["B1_cm"], params["jmax"])
+    diatom_Y = _rigid_rotor(params["B2_cm"], params["jmax"])
+    energies = np.array([5.0, 200.0, 800.0]) * CM
+    system = ticc.build_ScattSystem(diatom_X, diatom_Y, Jtot=params["J"], system_parity=1, potential=ticc.PESWrapper(interaction=interaction), reduced_mass=params["mu_amu"] * AMU)
+    _solve_and_save(
+        "solve_diatom_diatom",
+        params,
+        system,
+        params["boundaries"],
+        params["half_steps"],
+        energies,
+        "inelastic",
+        512.0,
+        n_theta_X=params["n_theta_X"],
+        n_theta_Y=params["n_theta_Y"],
+        n_phi=params["n_phi"],
+    )
+
+
+def make_channel_counts() -> None:
+    """Channel counts per (J, parity) from the reference's own channel builder."""
+    counts = {}
+    rigid = _rigid_rotor(20.0, 20)
+    for parity in (1, -1):
+        system = ticc.build_ScattSystem(ticc.AtomSpec(), rigid, Jtot=20, system_parity=parity)
+        counts[f"rigid_j20_J20_p{parity}"] = system.basis.n_channel
+    table = np.zeros((4, 31))
+    spec = ticc.DiatomSpec(Eint=table) if hasattr(ticc, "DiatomSpec") else None
+    from pyticc.basis.monomer import DiatomSpec
+
+    spec = DiatomSpec(Eint=table)
+    for J in (0, 1, 2, 15, 30, 45, 60):
+        for parity in (1, -1):
+            system = ticc.ScattSystem(ticc.AtomSpec(), spec, Jtot=J, system_parity=parity)
+            from pyticc.basis.channel import build_ChannelBasis
+
+            counts[f"vib_v3_j30_J{J}_p{parity}"] = build_ChannelBasis(system, ticc.ChannelSpec()).n_channel
+    pair = DiatomSpec(Eint=np.zeros((1, 9)))
+    for parity in (1, -1):
+        system = ticc.ScattSystem(pair, pair, Jtot=6, system_parity=parity)
+        counts[f"pair_j8_J6_p{parity}"] = build_ChannelBasis(system, ticc.ChannelSpec()).n_channel
+    slow = DiatomSpec(Eint=np.zeros((1, 41)))
+    for J in (0, 5, 10):
+        system = ticc.ScattSystem(ticc.AtomSpec(), slow, Jtot=J, system_parity=1)
+        counts[f"capture_j40_J{J}_p1"] = build_ChannelBasis(system, ticc.ChannelSpec()).n_channel
+    _save("channel_counts", counts)
+
+
+if __name__ == "__main__":
+    make_ldmd()
+    make_contract()
+    make_smatrix()
+    make_bessel()
+    make_grid()
+    make_solve_rigid()
+    make_solve_morse()
+    make_solve_diatom_diatom()
+    make_channel_counts()
