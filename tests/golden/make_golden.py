@@ -218,10 +218,40 @@ def _pad_smat(smats, n_channel):
     return out
 
 
+def _vbasis_rows(system, grid):
+    """The reference's own weighted contraction rows, grouped by K."""
+    from pyticc.matrix.interaction import atom_diatom as vmat_ad
+    from pyticc.matrix.interaction import diatom_diatom as vmat_dd
+
+    if grid.scattering_type is ticc.ScatteringType.ATOM_DIATOM:
+        vb = vmat_ad.prepare(system.basis, system.monomer_Y.rovib, grid.coordinate("cos_theta"), grid.weight("theta"))
+    else:
+        vb = vmat_dd.prepare(
+            system.basis,
+            system.monomer_X.rovib,
+            system.monomer_Y.rovib,
+            grid.coordinate("cos_theta_X"),
+            grid.weight("theta_X"),
+            grid.coordinate("cos_theta_Y"),
+            grid.weight("theta_Y"),
+            grid.coordinate("phi"),
+            grid.weight("phi"),
+        )
+    rows = {}
+    for K, indices in vb.channel_indices.items():
+        rows[f"vrows_idx_{K}"] = np.asarray(indices)
+        rows[f"vrows_real_{K}"] = vb.B_real[K]
+        if vb.B_imag is not None:
+            rows[f"vrows_imag_{K}"] = vb.B_imag[K]
+    rows["vrows_norm"] = np.asarray(vb.normalization)
+    return rows
+
+
 def _solve_and_save(name, params, system, boundaries, halves, energies, mode, memory_mb, **quad):
     grid = ticc.prepare_potential(system, boundaries, halves, **quad)
     result = ticc.solve(system, energies, grid, ticc.Propagation(mode=mode, memory_mb=memory_mb, device="cpu"))
     basis = system.basis
+    vrows = _vbasis_rows(system, grid)
     channels = np.asarray([[c.mis_X.j, -1 if c.mis_X.v is None else c.mis_X.v, c.mis_Y.j, -1 if c.mis_Y.v is None else c.mis_Y.v, c.j_couple, c.K] for c in basis])
     _save(
         name,
@@ -238,6 +268,8 @@ def _solve_and_save(name, params, system, boundaries, halves, energies, mode, me
         Smat=_pad_smat(result.Smat, basis.n_channel),
         n_open=np.asarray([m.shape[0] for m in result.Smat]),
         cos_theta=grid.coordinate("cos_theta") if grid.scattering_type is ticc.ScatteringType.ATOM_DIATOM else np.zeros(0),
+        half_steps_sectors=np.asarray([s.radial_half_step for s in grid.sectors]),
+        **vrows,
     )
 
 
