@@ -1,0 +1,136 @@
+/*
+ * ticc_b200 — C ABI of the B200 (sm_100a) coupled-channel scattering kernels.
+ *
+ * Every entry point is stream-ordered and non-blocking: it validates its
+ * arguments on the host, enqueues kernels on `stream` (a cudaStream_t passed as
+ * void*, NULL for the legacy default stream) and returns a status code.  All
+ * buffers are caller-owned device pointers; no entry point allocates device
+ * memory except the runtime's own one-time module state.  Scratch memory is a
+ * caller-provided `workspace` whose size comes from the matching *_workspace_size
+ * query.
+ *
+ * `device_status` (optional, may be NULL) points to int[4] of device memory that
+ * the caller zeroes before the call and reads after synchronising the stream:
+ * {code, batch item, detail, 0}.  Codes: 0 ok, 1 singular pivot block in a
+ * symmetric sweep (detail = block index), 2 non-finite output, 3 Bessel continued
+ * fraction did not converge (detail = channel), 4 energy exactly at a threshold,
+ * 5 more open channels than the caller's max_open.
+ *
+ * Matrices are row-major float64, or complex128 with interleaved (re, im) pairs
+ * when `is_complex` is set.  Symmetric inputs are required where noted: their
+ * antisymmetric part is ignored (the reference's callers only ever pass symmetric
+ * matrices; see each entry).
+ *
+ * Each declaration names the reference (PyTICC, src/pyticc/...) function it
+ * replaces; the Python host layer pyticc_b200 binds them through ctypes.
+ */
+#ifndef TICC_B200_H
+#define TICC_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  TICC_OK = 0,
+  TICC_ERR_INVALID_ARGUMENT = 1,
+  TICC_ERR_CUDA = 2,
+  TICC_ERR_WORKSPACE = 3,
+  TICC_ERR_UNSUPPORTED = 4
+};
+
+enum { TICC_PRECISION_FP64 = 0, TICC_PRECISION_MIXED = 1 };
+
+/* Library ABI version (major * 10000 + minor * 100 + patch). */
+int ticc_version(void);
+
+/* Copy the calling thread's most recent error message into buf (NUL-terminated).
+ * Returns the message length. */
+int ticc_last_error(char* buf, size_t len);
+
+/* ---- symmetric inversion ---------------------------------------------------
+ * Batched in-place inverse of symmetric (or complex symmetric) n x n matrices by
+ * a blocked sweep with 128-wide pivot blocks and partial pivoting inside each
+ * block.  Replaces the energy-shared jnp.linalg.solve(I - h^2 T_mid / 6, I) of
+ * _correction_matrices (propagation/logd.py:162) and is the kernel behind every
+ * inversion below.  M: batch x n x n at stride n*n (complex: interleaved). */
+int ticc_sym_inverse_workspace_size(int n, int batch, int is_complex, size_t* bytes);
+int ticc_sym_inverse(void* M, int n, int batch, int is_complex, void* workspace, size_t workspace_bytes, int* device_status, void* stream);
+
+/* ---- LDMD propagation -------------------------------------------------------
+ * Propagate n_energy log-derivative matrices Y through n_sector Manolopoulos LDMD
+ * sectors.  Replaces propagate_logD (propagation/logd.py:340-398) with its
+ * vmap/scan body _propagate_logD_jax (:288-330), _correction_matrices (:143-164),
+ * _reference_values (:98-132) and _propagate_with_corrections (:168-194).
+ *   Y          device, n_energy x n x n (complex interleaved if is_complex); read at
+ *              the first sector start, overwritten with Y at the last sector end.
+ *              Must be symmetric (the reference's initialisers are diagonal).
+ *   energies   device, n_energy total energies (hartree).
+ *   half_steps device, n_sector half-steps (bohr), all > 0.
+ *   W_start/W_mid/W_end device, energy-independent W_base at the sector start,
+ *              midpoint and end, each n x n (symmetric) at the given element stride
+ *              between consecutive sectors (e.g. 2*n*n for an interleaved point list).
+ *   precision  TICC_PRECISION_FP64 (all-FP64) or TICC_PRECISION_MIXED. */
+int ticc_ldmd_workspace_size(int n_channel, int n_energy, int n_sector, int is_complex, int precision, size_t* bytes);
+int ticc_ldmd_propagate(void* Y, int is_complex, const double* energies, int n_energy, double reduced_mass, const double* half_steps,
+                        const double* W_start, long long W_start_stride, const double* W_mid, long long W_mid_stride, const double* W_end,
+                        long long W_end_stride, int n_sector, int n_channel, int precision, void* workspace, size_t workspace_bytes,
+                        int* device_status, void* stream);
+
+/* ---- PotentialGrid contraction and W assembly --------------------------------
+ * V_K(R) = norm [(B_r v(R)) B_r^T + (B_i v(R)) B_i^T] per K group, scattered into the
+ * (n_R, n_channel, n_channel) block-diagonal V.  Replaces contract_device /
+ * _contract_block_device (matrix/interaction/common.py:153-211, :66-74).  With U
+ * non-NULL the output is instead W_base(R) = U/R^2 + 2 mu [V(R) + diag(E_int)], the
+ * device W assembly of propagation/runner.py:265-271.
+ *   rows_real/rows_imag  device, n_rows x n_grid weighted basis rows, grouped by K:
+ *                        group g owns rows [group_offsets[g], group_offsets[g+1]).
+ *   group_offsets        HOST array of n_groups + 1 non-decreasing row offsets.
+ *   row_out              device, output channel position of every row.
+ *   potential            device, n_R rows of n_grid values at row stride pot_stride.
+ *   radial_points        device, n_R values (used only when U != NULL).
+ *   out                  device, n_R x n_channel x n_channel. */
+int ticc_contract(const double* rows_real, const double* rows_imag, const int* group_offsets, int n_groups, const int* row_out, int n_grid,
+                  double normalization, const double* potential, long long pot_stride, int n_R, int n_channel, const double* radial_points,
+                  const double* U, const double* E_int, double reduced_mass, double* out, void* stream);
+
+/* ---- BF -> SF transform --------------------------------------------------------
+ * Y_SF = B^T Y_BF B for a batch.  Replaces transform_logD_BF_to_SF
+ * (match/asymptotic.py:82-110).  Y, Y_out: batch x n x n (complex interleaved if
+ * is_complex; in-place allowed); B: n x n real. */
+int ticc_transform_workspace_size(int n, int batch, int is_complex, size_t* bytes);
+int ticc_transform_bf_to_sf(const void* Y, void* Y_out, const double* B, int n, int batch, int is_complex, void* workspace, size_t workspace_bytes,
+                            void* stream);
+
+/* ---- Riccati-Bessel functions --------------------------------------------------
+ * out[4*i .. 4*i+3] = (j, n, j', n') of order ell[i] at x[i] (nu = ell + 1/2).
+ * Replaces riccati_bessel_jy (match/bessel.py:7-45). */
+int ticc_riccati_bessel_jy(const double* ell, const double* x, int n, double* out, int* device_status, void* stream);
+
+/* out[i] = K'_nu(x)/K_nu(x) = -K_{nu-1}(x)/K_nu(x) - nu/x.
+ * Replaces modified_bessel_K_logD (match/bessel.py:90-122). */
+int ticc_bessel_k_logd(const double* nu, const double* x, int n, double* out, int* device_status, void* stream);
+
+/* ---- asymptotic matching --------------------------------------------------------
+ * S matrices from SF log-derivatives.  Replaces get_Smat (match/smatrix.py:139-223)
+ * with _reference_functions (:10-79) and _open_reaction_matrix (:86-132).
+ *   Y       device, n_energy x n x n SF log-derivatives (complex if is_complex), symmetric.
+ *   E_int, L, energies  device.
+ *   S       device, n_energy x n x n complex128: S[e] holds the n_open[e] x n_open[e]
+ *           S matrix in its top-left corner, rows/columns in the order of
+ *           flatnonzero(E_int < energy); the rest is zero.
+ *   n_open  device, n_energy ints.
+ *   max_open host bound on the open-channel count at every energy (the caller knows
+ *           E_int and the energies); a larger count sets device status 5. */
+int ticc_match_workspace_size(int n_channel, int n_energy, int is_complex, int max_open, size_t* bytes);
+int ticc_match_smatrix(const void* Y, int is_complex, double Rmatch, const double* energies, int n_energy, double reduced_mass, const double* E_int,
+                       const double* L, int n_channel, int max_open, double* S, int* n_open, void* workspace, size_t workspace_bytes,
+                       int* device_status, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TICC_B200_H */

@@ -1,0 +1,338 @@
+// extern "C" entry points of libticc_b200.so (declared in include/ticc_b200.h).
+//
+// Each entry validates its arguments on the host, carves the caller's workspace into
+// 256-byte aligned regions, enqueues the kernels on the caller's stream and returns a
+// status code; the message of the last failure is kept per host thread.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "../../include/ticc_b200.h"
+#include "contract.cuh"
+#include "gemm.cuh"
+#include "ldmd.cuh"
+#include "match.cuh"
+#include "sweep.cuh"
+
+namespace {
+
+thread_local char g_message[512] = "";
+
+int fail(int code, const char* fmt, ...) {
+  va_list args;
+  va_start(args, fmt);
+  vsnprintf(g_message, sizeof(g_message), fmt, args);
+  va_end(args);
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) { return fail(TICC_ERR_CUDA, "%s: %s", where, cudaGetErrorString(e)); }
+
+// Bump allocator over the caller's workspace (256-byte aligned regions).
+struct Carver {
+  char* base;
+  size_t used = 0;
+  template <class T>
+  T* take(size_t count) {
+    used = (used + 255) & ~size_t(255);
+    T* p = base ? reinterpret_cast<T*>(base + used) : nullptr;
+    used += count * sizeof(T);
+    return p;
+  }
+};
+
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+size_t ldmd_layout(ticc::LdmdLayout& L, int n, int n_energy, int n_sector, int is_complex, char* base) {
+  Carver c{base};
+  L.n = n;
+  L.n_energy = n_energy;
+  L.is_complex = is_complex;
+  L.np = ticc::ldmd_np(n, is_complex);
+  L.npr = ticc::ldmd_np(n, 0);
+  L.M = c.take<double>((size_t)n_energy * L.np * L.np);
+  L.Qm = c.take<double>((size_t)n_sector * L.npr * L.npr);
+  L.y1 = c.take<double>((size_t)n_sector * n_energy * n);
+  L.y2 = c.take<double>((size_t)n_sector * n_energy * n);
+  // one scratch region serves the per-energy sweeps and the per-sector Q_mid sweeps
+  // (the latter are chunked to fit); at least one sector's worth is guaranteed
+  const size_t need_e = (size_t)n_energy * ticc::sweep_scratch_doubles(L.np);
+  const size_t need_s = ticc::sweep_scratch_doubles(L.npr) * (size_t)(n_sector < 8 ? n_sector : 8);
+  L.scratch_doubles = need_e > need_s ? need_e : need_s;
+  L.scratch = c.take<double>(L.scratch_doubles);
+  return c.used + 256;
+}
+
+size_t match_layout(ticc::MatchLayout& L, int n, int n_energy, int is_complex, int max_open, char* base) {
+  Carver c{base};
+  L.n = n;
+  L.n_energy = n_energy;
+  L.is_complex = is_complex;
+  L.max_open = max_open;
+  L.npz = ticc::ldmd_np(n, is_complex);
+  L.npa = (int)ticc::round_up(2LL * (max_open > 0 ? max_open : 1), ticc::kBlock);
+  L.Jv = c.take<double>((size_t)n_energy * n);
+  L.Nv = c.take<double>((size_t)n_energy * n);
+  L.Jp = c.take<double>((size_t)n_energy * n);
+  L.Np = c.take<double>((size_t)n_energy * n);
+  L.gamma = c.take<double>((size_t)n_energy * n);
+  L.oidx = c.take<int>((size_t)n_energy * n);
+  L.Z = c.take<double>((size_t)n_energy * L.npz * L.npz);
+  L.A = c.take<double>((size_t)n_energy * L.npa * L.npa);
+  L.B = c.take<double>((size_t)n_energy * L.npa * L.npa);
+  L.C = c.take<double>((size_t)n_energy * L.npa * L.npa);
+  const int np = L.npz > L.npa ? L.npz : L.npa;
+  L.scratch = c.take<double>((size_t)n_energy * ticc::sweep_scratch_doubles(np));
+  return c.used + 256;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ticc_version(void) { return 10000; }
+
+int ticc_last_error(char* buf, size_t len) {
+  const size_t n = strlen(g_message);
+  if (buf && len) {
+    strncpy(buf, g_message, len - 1);
+    buf[len - 1] = '\0';
+  }
+  return (int)n;
+}
+
+// ---- symmetric inversion ---------------------------------------------------------------
+static size_t sym_layout(int n, int batch, int is_complex, double** M, double** scratch, char* base) {
+  Carver c{base};
+  const int np = ticc::ldmd_np(n, is_complex);
+  *M = c.take<double>((size_t)batch * np * np);
+  *scratch = c.take<double>((size_t)batch * ticc::sweep_scratch_doubles(np));
+  return c.used + 256;
+}
+
+int ticc_sym_inverse_workspace_size(int n, int batch, int is_complex, size_t* bytes) {
+  if (n < 1 || batch < 1 || bytes == nullptr) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_sym_inverse_workspace_size: n=%d batch=%d", n, batch);
+  double *M, *s;
+  *bytes = sym_layout(n, batch, is_complex, &M, &s, nullptr);
+  return TICC_OK;
+}
+
+__global__ void sym_load_kernel(const double* src, int n, int is_complex, double* M, int np) {
+  const int b = blockIdx.y;
+  const int nl = is_complex ? np / 2 : np;
+  double* Mb = M + (long long)b * np * np;
+  const double* s = src + (long long)b * n * n * (is_complex ? 2 : 1);
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < (long long)nl * nl; idx += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / nl), j = (int)(idx % nl);
+    if (i >= n || j >= n) {
+      if (is_complex) {
+        for (int a = 0; a < 2; ++a)
+          for (int c = 0; c < 2; ++c) ticc::put_padding(Mb, np, 2LL * i + a, 2LL * j + c);
+      } else {
+        ticc::put_padding(Mb, np, i, j);
+      }
+      continue;
+    }
+    double x, z = 0.0;
+    if (is_complex) {
+      x = 0.5 * (s[2 * ((long long)i * n + j)] + s[2 * ((long long)j * n + i)]);
+      z = 0.5 * (s[2 * ((long long)i * n + j) + 1] + s[2 * ((long long)j * n + i) + 1]);
+    } else {
+      x = 0.5 * (s[(long long)i * n + j] + s[(long long)j * n + i]);
+    }
+    ticc::put_element(Mb, np, i, j, x, z, is_complex);
+  }
+}
+
+__global__ void sym_store_kernel(const double* M, int np, double* dst, int n, int is_complex) {
+  const int b = blockIdx.y;
+  const double* Mb = M + (long long)b * np * np;
+  double* d = dst + (long long)b * n * n * (is_complex ? 2 : 1);
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < (long long)n * n; idx += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / n), j = (int)(idx % n);
+    double sr, si;
+    ticc::get_swept(Mb, np, i, j, is_complex, sr, si);
+    if (is_complex) {
+      d[2 * idx] = -sr;
+      d[2 * idx + 1] = -si;
+    } else {
+      d[idx] = -sr;
+    }
+  }
+}
+
+int ticc_sym_inverse(void* M, int n, int batch, int is_complex, void* workspace, size_t workspace_bytes, int* device_status, void* stream) {
+  if (M == nullptr || n < 1 || batch < 1) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_sym_inverse: M=%p n=%d batch=%d", M, n, batch);
+  double *Mw, *scratch;
+  const size_t need = sym_layout(n, batch, is_complex, &Mw, &scratch, nullptr);
+  if (workspace == nullptr || workspace_bytes < need) return fail(TICC_ERR_WORKSPACE, "ticc_sym_inverse: workspace of %zu bytes given, %zu needed", workspace_bytes, need);
+  sym_layout(n, batch, is_complex, &Mw, &scratch, static_cast<char*>(workspace));
+  const int np = ticc::ldmd_np(n, is_complex);
+  const long long nl = is_complex ? np / 2 : np;
+  cudaStream_t s = as_stream(stream);
+  sym_load_kernel<<<dim3(ticc::grid_for(nl * nl, 256, 8192), batch), 256, 0, s>>>(static_cast<double*>(M), n, is_complex, Mw, np);
+  cudaError_t e = ticc::sweep_sym(Mw, (long long)np * np, np, batch, scratch, device_status, s);
+  if (e != cudaSuccess) return cuda_fail(e, "ticc_sym_inverse");
+  sym_store_kernel<<<dim3(ticc::grid_for((long long)n * n, 256, 8192), batch), 256, 0, s>>>(Mw, np, static_cast<double*>(M), n, is_complex);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_sym_inverse");
+}
+
+// ---- LDMD propagation ----------------------------------------------------------------------
+int ticc_ldmd_workspace_size(int n_channel, int n_energy, int n_sector, int is_complex, int precision, size_t* bytes) {
+  if (n_channel < 1 || n_energy < 1 || n_sector < 1 || bytes == nullptr)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_ldmd_workspace_size: n_channel=%d n_energy=%d n_sector=%d", n_channel, n_energy, n_sector);
+  if (precision != TICC_PRECISION_FP64) return fail(TICC_ERR_UNSUPPORTED, "ticc_ldmd_workspace_size: precision mode %d is not available", precision);
+  ticc::LdmdLayout L{};
+  *bytes = ldmd_layout(L, n_channel, n_energy, n_sector, is_complex, nullptr);
+  return TICC_OK;
+}
+
+int ticc_ldmd_propagate(void* Y, int is_complex, const double* energies, int n_energy, double reduced_mass, const double* half_steps, const double* W_start,
+                        long long W_start_stride, const double* W_mid, long long W_mid_stride, const double* W_end, long long W_end_stride, int n_sector,
+                        int n_channel, int precision, void* workspace, size_t workspace_bytes, int* device_status, void* stream) {
+  if (Y == nullptr || energies == nullptr || half_steps == nullptr || W_start == nullptr || W_mid == nullptr || W_end == nullptr)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_ldmd_propagate: null input pointer");
+  if (n_channel < 1 || n_energy < 1 || n_sector < 1)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_ldmd_propagate: n_channel=%d n_energy=%d n_sector=%d must be positive", n_channel, n_energy, n_sector);
+  if (!(reduced_mass > 0.0)) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_ldmd_propagate: reduced_mass must be positive, got %g", reduced_mass);
+  if (precision != TICC_PRECISION_FP64) return fail(TICC_ERR_UNSUPPORTED, "ticc_ldmd_propagate: precision mode %d is not available", precision);
+  ticc::LdmdLayout L{};
+  const size_t need = ldmd_layout(L, n_channel, n_energy, n_sector, is_complex, nullptr);
+  if (workspace == nullptr || workspace_bytes < need) return fail(TICC_ERR_WORKSPACE, "ticc_ldmd_propagate: workspace of %zu bytes given, %zu needed", workspace_bytes, need);
+  ldmd_layout(L, n_channel, n_energy, n_sector, is_complex, static_cast<char*>(workspace));
+  ticc::LdmdSectors sec{half_steps, W_start, W_mid, W_end, W_start_stride, W_mid_stride, W_end_stride, n_sector};
+  cudaError_t e = ticc::ldmd_propagate(static_cast<double*>(Y), energies, reduced_mass, sec, L, device_status, as_stream(stream));
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_ldmd_propagate");
+}
+
+// ---- contraction ---------------------------------------------------------------------------------
+int ticc_contract(const double* rows_real, const double* rows_imag, const int* group_offsets, int n_groups, const int* row_out, int n_grid,
+                  double normalization, const double* potential, long long pot_stride, int n_R, int n_channel, const double* radial_points, const double* U,
+                  const double* E_int, double reduced_mass, double* out, void* stream) {
+  if (rows_real == nullptr || group_offsets == nullptr || row_out == nullptr || potential == nullptr || out == nullptr)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_contract: null input pointer");
+  if (n_groups < 0 || n_grid < 1 || n_R < 0 || n_channel < 1 || pot_stride < n_grid)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_contract: n_groups=%d n_grid=%d n_R=%d n_channel=%d pot_stride=%lld", n_groups, n_grid, n_R, n_channel, pot_stride);
+  if (U != nullptr && (radial_points == nullptr || E_int == nullptr || !(reduced_mass > 0.0)))
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_contract: W assembly needs radial_points, E_int and a positive reduced_mass");
+  for (int g = 0; g < n_groups; ++g)
+    if (group_offsets[g + 1] < group_offsets[g]) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_contract: group_offsets must be non-decreasing");
+  if (n_R == 0) return TICC_OK;
+  cudaStream_t s = as_stream(stream);
+  ticc::contract_init_kernel<<<ticc::grid_for((long long)n_R * n_channel * n_channel, 256), 256, 0, s>>>(out, n_channel, n_R, radial_points, U, E_int, reduced_mass);
+  const double scale = normalization * (U != nullptr ? 2.0 * reduced_mass : 1.0);
+  for (int g = 0; g < n_groups; ++g) {
+    const int rows = group_offsets[g + 1] - group_offsets[g];
+    if (rows == 0) continue;
+    const int t = (rows + ticc::kCTile - 1) / ticc::kCTile;
+    ticc::contract_group_kernel<<<dim3(t * (t + 1) / 2, n_R), 256, 0, s>>>(rows_real, rows_imag, group_offsets[g], rows, row_out, n_grid, scale, potential, pot_stride, n_channel, out);
+  }
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_contract");
+}
+
+// ---- BF -> SF transform ------------------------------------------------------------------------------
+static size_t transform_layout(int n, int batch, double** Bp, double** P, double** T, char* base) {
+  Carver c{base};
+  const int np = ticc::ldmd_np(n, 0);
+  *Bp = c.take<double>((size_t)np * np);
+  *P = c.take<double>((size_t)batch * np * np);
+  *T = c.take<double>((size_t)batch * np * np);
+  return c.used + 256;
+}
+
+int ticc_transform_workspace_size(int n, int batch, int is_complex, size_t* bytes) {
+  if (n < 1 || batch < 1 || bytes == nullptr) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_transform_workspace_size: n=%d batch=%d", n, batch);
+  double *a, *b, *c;
+  *bytes = transform_layout(n, batch, &a, &b, &c, nullptr);
+  return TICC_OK;
+}
+
+int ticc_transform_bf_to_sf(const void* Y, void* Y_out, const double* B, int n, int batch, int is_complex, void* workspace, size_t workspace_bytes, void* stream) {
+  if (Y == nullptr || Y_out == nullptr || B == nullptr || n < 1 || batch < 1) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_transform_bf_to_sf: bad arguments");
+  double *Bp, *P, *T;
+  const size_t need = transform_layout(n, batch, &Bp, &P, &T, nullptr);
+  if (workspace == nullptr || workspace_bytes < need) return fail(TICC_ERR_WORKSPACE, "ticc_transform_bf_to_sf: workspace of %zu bytes given, %zu needed", workspace_bytes, need);
+  transform_layout(n, batch, &Bp, &P, &T, static_cast<char*>(workspace));
+  const int np = ticc::ldmd_np(n, 0);
+  cudaStream_t s = as_stream(stream);
+  const long long area = (long long)np * np;
+  ticc::pad_plane_kernel<<<dim3(ticc::grid_for(area, 256, 8192), 1), 256, 0, s>>>(B, n, 0, 0, Bp, np);
+  for (int part = 0; part < (is_complex ? 2 : 1); ++part) {
+    ticc::pad_plane_kernel<<<dim3(ticc::grid_for(area, 256, 8192), batch), 256, 0, s>>>(static_cast<const double*>(Y), n, is_complex, part, P, np);
+    // T^T = (B^T Y)^T, then (B^T T^T)^T = T B = B^T Y B
+    ticc::GemmBatch g1{Bp, np, 0, P, np, area, T, np, area, np, 1.0, 1};
+    cudaError_t e = ticc::gemm_tn(g1, np, np, batch, s);
+    if (e != cudaSuccess) return cuda_fail(e, "ticc_transform_bf_to_sf");
+    ticc::GemmBatch g2{Bp, np, 0, T, np, area, P, np, area, np, 1.0, 1};
+    e = ticc::gemm_tn(g2, np, np, batch, s);
+    if (e != cudaSuccess) return cuda_fail(e, "ticc_transform_bf_to_sf");
+    ticc::unpad_plane_kernel<<<dim3(ticc::grid_for((long long)n * n, 256, 8192), batch), 256, 0, s>>>(P, np, static_cast<double*>(Y_out), n, is_complex, part);
+  }
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_transform_bf_to_sf");
+}
+
+// ---- Bessel functions -------------------------------------------------------------------------------------
+__global__ void riccati_kernel(const double* ell, const double* x, int n, double* out, int* status) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const ticc::BesselJY r = ticc::riccati_bessel(ell[i], x[i]);
+    if (!r.ok) ticc::report_status(status, ticc::kDeviceBesselFailed, 0, i);
+    out[4 * i] = r.J;
+    out[4 * i + 1] = r.Y;
+    out[4 * i + 2] = r.Jp;
+    out[4 * i + 3] = r.Yp;
+  }
+}
+
+__global__ void k_logd_kernel(const double* nu, const double* x, int n, double* out, int* status) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = ticc::bessel_k_logd(nu[i], x[i]);
+    if (!isfinite(v)) ticc::report_status(status, ticc::kDeviceBesselFailed, 0, i);
+    out[i] = v;
+  }
+}
+
+int ticc_riccati_bessel_jy(const double* ell, const double* x, int n, double* out, int* device_status, void* stream) {
+  if (ell == nullptr || x == nullptr || out == nullptr || n < 0) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_riccati_bessel_jy: bad arguments");
+  if (n == 0) return TICC_OK;
+  riccati_kernel<<<ticc::grid_for(n, 128), 128, 0, as_stream(stream)>>>(ell, x, n, out, device_status);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_riccati_bessel_jy");
+}
+
+int ticc_bessel_k_logd(const double* nu, const double* x, int n, double* out, int* device_status, void* stream) {
+  if (nu == nullptr || x == nullptr || out == nullptr || n < 0) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_bessel_k_logd: bad arguments");
+  if (n == 0) return TICC_OK;
+  k_logd_kernel<<<ticc::grid_for(n, 128), 128, 0, as_stream(stream)>>>(nu, x, n, out, device_status);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_bessel_k_logd");
+}
+
+// ---- matching ---------------------------------------------------------------------------------------------
+int ticc_match_workspace_size(int n_channel, int n_energy, int is_complex, int max_open, size_t* bytes) {
+  if (n_channel < 1 || n_energy < 1 || max_open < 0 || max_open > n_channel || bytes == nullptr)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_match_workspace_size: n_channel=%d n_energy=%d max_open=%d", n_channel, n_energy, max_open);
+  ticc::MatchLayout L{};
+  *bytes = match_layout(L, n_channel, n_energy, is_complex, max_open, nullptr);
+  return TICC_OK;
+}
+
+int ticc_match_smatrix(const void* Y, int is_complex, double Rmatch, const double* energies, int n_energy, double reduced_mass, const double* E_int, const double* L,
+                       int n_channel, int max_open, double* S, int* n_open, void* workspace, size_t workspace_bytes, int* device_status, void* stream) {
+  if (Y == nullptr || energies == nullptr || E_int == nullptr || L == nullptr || S == nullptr || n_open == nullptr)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_match_smatrix: null input pointer");
+  if (n_channel < 1 || n_energy < 1 || max_open < 0 || max_open > n_channel)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_match_smatrix: n_channel=%d n_energy=%d max_open=%d", n_channel, n_energy, max_open);
+  if (!(Rmatch > 0.0) || !(reduced_mass > 0.0))
+    return fail(TICC_ERR_INVALID_ARGUMENT, "Rmatch and reduced_mass must be positive, but got Rmatch=%g, reduced_mass=%g", Rmatch, reduced_mass);
+  ticc::MatchLayout Lay{};
+  const size_t need = match_layout(Lay, n_channel, n_energy, is_complex, max_open, nullptr);
+  if (workspace == nullptr || workspace_bytes < need) return fail(TICC_ERR_WORKSPACE, "ticc_match_smatrix: workspace of %zu bytes given, %zu needed", workspace_bytes, need);
+  match_layout(Lay, n_channel, n_energy, is_complex, max_open, static_cast<char*>(workspace));
+  cudaError_t e = ticc::match_smatrix(static_cast<const double*>(Y), Rmatch, energies, reduced_mass, E_int, L, S, n_open, Lay, device_status, as_stream(stream));
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_match_smatrix");
+}
+
+}  // extern "C"

@@ -1,0 +1,119 @@
+// FP64 tensor-core tile core: one CTA computes a 128x128 tile of A^T B with
+// mma.sync m8n8k4 f64 (DMMA), operands staged into shared memory by cp.async.
+//
+// B200 has no tcgen05 kind for FP64; the FP64 tensor pipe is reached through the
+// warp-level DMMA instruction.  A CTA of 8 warps (2 x 4) owns a 128 x 128 tile, each
+// warp a 64 x 32 sub-tile held as 8 x 4 DMMA accumulators (64 doubles per lane).
+// Operands are "k-major": row k of A holds A^T[k][m0 .. m0+127], which is how every
+// caller stores them (the sweep's panels are rows of a symmetric matrix).
+#pragma once
+
+#include "ticc_common.cuh"
+
+namespace ticc {
+
+constexpr size_t kTileSmemBytes = size_t(4) * kChunk * kStride * sizeof(double);  // 135168
+
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+struct TileAcc {
+  double v[8][4][2];
+};
+
+// Stage rows [k, k + kChunk) of a k-major operand (128 contiguous doubles per row).
+__device__ __forceinline__ void stage_rows(double* dst, const double* src, long long ld, int k, int tid) {
+#pragma unroll
+  for (int i = 0; i < (kChunk * 64) / kGemmThreads; ++i) {
+    const int piece = tid + i * kGemmThreads;
+    const int r = piece >> 6;
+    const int c = (piece & 63) * 2;
+    cp_async16(dst + r * kStride + c, src + (long long)(k + r) * ld + c);
+  }
+}
+
+__device__ __forceinline__ void mma_chunk(TileAcc& acc, const double* As, const double* Bs, int warp, int lane) {
+  const int wm = (warp >> 2) * 64;
+  const int wn = (warp & 3) * 32;
+  const int kr = lane & 3;
+  const int mr = lane >> 2;
+#pragma unroll
+  for (int kk = 0; kk < kChunk; kk += 4) {
+    double a[8], b[4];
+    const double* arow = As + (kk + kr) * kStride + wm + mr;
+    const double* brow = Bs + (kk + kr) * kStride + wn + mr;
+#pragma unroll
+    for (int mt = 0; mt < 8; ++mt) a[mt] = arow[mt * 8];
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) b[nt] = brow[nt * 8];
+#pragma unroll
+    for (int mt = 0; mt < 8; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) dmma_8x8x4(acc.v[mt][nt], a[mt], b[nt]);
+  }
+}
+
+// acc = sum_{k < K} A[k][0..127]^T B[k][0..127]; A, B already offset to their tile column.
+// K must be a multiple of kChunk.  Ends with a __syncthreads(), so smem is free afterwards.
+__device__ inline void tile_gemm_tn(TileAcc& acc, const double* A, long long lda, const double* B, long long ldb, int K, double* smem) {
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+#pragma unroll
+  for (int mt = 0; mt < 8; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) acc.v[mt][nt][0] = acc.v[mt][nt][1] = 0.0;
+
+  double* As[2] = {smem, smem + 2 * kChunk * kStride};
+  double* Bs[2] = {smem + kChunk * kStride, smem + 3 * kChunk * kStride};
+  const int nchunks = K / kChunk;
+  stage_rows(As[0], A, lda, 0, tid);
+  stage_rows(Bs[0], B, ldb, 0, tid);
+  cp_async_commit();
+  for (int c = 0; c < nchunks; ++c) {
+    if (c + 1 < nchunks) {
+      stage_rows(As[(c + 1) & 1], A, lda, (c + 1) * kChunk, tid);
+      stage_rows(Bs[(c + 1) & 1], B, ldb, (c + 1) * kChunk, tid);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    mma_chunk(acc, As[c & 1], Bs[c & 1], warp, lane);
+    __syncthreads();
+  }
+}
+
+// Write the accumulator into a [128][kStride] shared tile: Cs[row][col] = scale * acc.
+__device__ __forceinline__ void acc_to_smem(const TileAcc& acc, double* Cs, double scale) {
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  const int wm = (warp >> 2) * 64;
+  const int wn = (warp & 3) * 32;
+#pragma unroll
+  for (int mt = 0; mt < 8; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      const int row = wm + mt * 8 + (lane >> 2);
+      const int col = wn + nt * 8 + 2 * (lane & 3);
+      Cs[row * kStride + col] = scale * acc.v[mt][nt][0];
+      Cs[row * kStride + col + 1] = scale * acc.v[mt][nt][1];
+    }
+}
+
+}  // namespace ticc

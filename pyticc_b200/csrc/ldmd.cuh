@@ -1,0 +1,252 @@
+// LDMD log-derivative propagation (two half-steps per sector, diagonal reference
+// potential at the sector midpoint), batched over energies, driven sector by sector.
+//
+// Per sector s with half-step h, ref = diag(W_mid), p^2 = ref - 2 mu E:
+//   y1 = p coth(ph) | |p| cot(|p|h),  y2 = p csch(ph) | |p| csc(|p|h)   (series if |ph| < 1e-5)
+//   Q_start = h (W_start - diag ref)/3,  Q_end = h (W_end - diag ref)/3,
+//   Q_mid = (4/h) [(I - h^2 (W_mid - diag ref)/6)^{-1} - I]        (energy independent)
+//   Y_mid = Q_mid + y1 - y2 (Y + Q_start + y1)^{-1} y2
+//   Y_end = Q_end + y1 - y2 (Y_mid + Q_mid + y1)^{-1} y2
+// The sweep returns S = -A^{-1}, so "- y2 A^{-1} y2" is "+ y2 S y2": every step
+// between two inversions is one fused elementwise pass over the work matrices.
+#pragma once
+
+#include "sweep.cuh"
+#include "ticc_common.cuh"
+
+namespace ticc {
+
+struct LdmdSectors {
+  const double* h;        // [n_sector] half-steps (device)
+  const double* Ws;       // W_base at sector starts, sector stride ws_stride, row stride n
+  const double* Wm;
+  const double* We;
+  long long ws_stride, wm_stride, we_stride;
+  int n_sector;
+};
+
+struct LdmdLayout {
+  int n;          // logical channels
+  int n_energy;
+  int is_complex;
+  int np;         // padded sweep size of the per-energy work matrix
+  int npr;        // padded sweep size of the real, energy-shared Q_mid matrix
+  double* M;      // [n_energy][np][np]
+  double* Qm;     // [n_sector][npr][npr]
+  double* y1;     // [n_sector][n_energy][n]
+  double* y2;
+  double* scratch;
+  size_t scratch_doubles;
+};
+
+inline int ldmd_np(int n, int is_complex) { return (int)round_up((long long)(is_complex ? 2 * n : n), kBlock); }
+
+__device__ __forceinline__ void reference_pair(double h, double p2, double& y1, double& y2) {
+  const double mag = sqrt(fabs(p2));
+  const double arg = mag * h;
+  if (fabs(arg) < 1.0e-5) {
+    y1 = 1.0 / h + p2 * h / 3.0 - p2 * p2 * h * h * h / 45.0;
+    y2 = 1.0 / h - p2 * h / 6.0 + 7.0 * p2 * p2 * h * h * h / 360.0;
+  } else if (p2 >= 0.0) {
+    y1 = mag / tanh(arg);
+    y2 = mag / sinh(arg);
+  } else {
+    y1 = mag / tan(arg);
+    y2 = mag / sin(arg);
+  }
+}
+
+// y1/y2 for every (sector, energy, channel).
+__global__ void ldmd_reference_kernel(LdmdSectors sec, const double* energies, double mu, int n, int n_energy, double* y1, double* y2) {
+  const long long total = (long long)sec.n_sector * n_energy * n;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total; idx += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx % n);
+    const long long se = idx / n;
+    const int e = (int)(se % n_energy);
+    const int s = (int)(se / n_energy);
+    const double ref = sec.Wm[s * sec.wm_stride + (long long)i * n + i];
+    double a, b;
+    reference_pair(sec.h[s], ref - 2.0 * mu * energies[e], a, b);
+    y1[idx] = a;
+    y2[idx] = b;
+  }
+}
+
+__device__ __forceinline__ double sym(const double* W, int n, int i, int j) { return 0.5 * (W[(long long)i * n + j] + W[(long long)j * n + i]); }
+
+// Mq = I - h^2 (W_mid - diag ref)/6 (padded identity), batched over sectors.
+__global__ void ldmd_qmid_build_kernel(LdmdSectors sec, int n, int npr, double* Qm) {
+  const int s = blockIdx.y;
+  const double h = sec.h[s];
+  const double* Wm = sec.Wm + s * sec.wm_stride;
+  double* Q = Qm + (long long)s * npr * npr;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < (long long)npr * npr; idx += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / npr), j = (int)(idx % npr);
+    double v;
+    if (i < n && j < n) {
+      v = (i == j) ? 1.0 : -h * h * sym(Wm, n, i, j) / 6.0;
+    } else {
+      v = (i == j) ? 1.0 : 0.0;
+    }
+    Q[idx] = v;
+  }
+}
+
+// Q_mid = (4/h)(X - I) from the swept matrix -X.
+__global__ void ldmd_qmid_finish_kernel(LdmdSectors sec, int n, int npr, double* Qm) {
+  const int s = blockIdx.y;
+  const double h = sec.h[s];
+  double* Q = Qm + (long long)s * npr * npr;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < (long long)npr * npr; idx += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / npr), j = (int)(idx % npr);
+    Q[idx] = (i < n && j < n) ? 4.0 / h * (-Q[idx] - (i == j ? 1.0 : 0.0)) : 0.0;
+  }
+}
+
+// Store one logical element (X + iZ) of a work matrix, or padding.
+__device__ __forceinline__ void put_element(double* Mb, int np, int i, int j, double x, double z, int is_complex) {
+  if (is_complex) {
+    Mb[(long long)(2 * i) * np + 2 * j] = x;
+    Mb[(long long)(2 * i) * np + 2 * j + 1] = z;
+    Mb[(long long)(2 * i + 1) * np + 2 * j] = z;
+    Mb[(long long)(2 * i + 1) * np + 2 * j + 1] = -x;
+  } else {
+    Mb[(long long)i * np + j] = x;
+  }
+}
+
+// Read the swept value S = -A^{-1} at logical (i, j): real part S00 and the imaginary
+// companion -S01 (so that -A^{-1} = s_re + i s_im).
+__device__ __forceinline__ void get_swept(const double* Mb, int np, int i, int j, int is_complex, double& s_re, double& s_im) {
+  if (is_complex) {
+    s_re = Mb[(long long)(2 * i) * np + 2 * j];
+    s_im = -Mb[(long long)(2 * i) * np + 2 * j + 1];
+  } else {
+    s_re = Mb[(long long)i * np + j];
+    s_im = 0.0;
+  }
+}
+
+// Work-matrix padding: identity on the padded diagonal of the real sweep matrix.
+__device__ __forceinline__ void put_padding(double* Mb, int np, long long r, long long c) { Mb[r * np + c] = (r == c) ? 1.0 : 0.0; }
+
+// phase 0: A = Y_in + Q_start + y1          (first sector of the call)
+// phase 1: A = [Q_end' + y1' + y2' S y2'] + Q_start + y1   (S from the previous sector)
+// phase 2: B = 2 Q_mid + 2 y1 + y2 S y2
+// phase 3: Y_out = Q_end + y1 + y2 S y2     (last sector of the call)
+__global__ void ldmd_elementwise_kernel(int phase, int s, LdmdSectors sec, LdmdLayout L, const double* Yin, double* Yout) {
+  const int e = blockIdx.y;
+  const int n = L.n, np = L.np;
+  const int nl = L.is_complex ? np / 2 : np;  // logical-element grid covering the padded matrix
+  double* Mb = L.M + (long long)e * np * np;
+  const double h = sec.h[s];
+  const double* y1 = L.y1 + ((long long)s * L.n_energy + e) * n;
+  const double* y2 = L.y2 + ((long long)s * L.n_energy + e) * n;
+  const double* Ws = sec.Ws + s * sec.ws_stride;
+  const double* Wm = sec.Wm + s * sec.wm_stride;
+  const double* We = sec.We + s * sec.we_stride;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < (long long)nl * nl; idx += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / nl), j = (int)(idx % nl);
+    if (i >= n || j >= n) {
+      if (phase == 3) continue;
+      if (L.is_complex) {
+        for (int a = 0; a < 2; ++a)
+          for (int b = 0; b < 2; ++b) put_padding(Mb, np, 2LL * i + a, 2LL * j + b);
+      } else {
+        put_padding(Mb, np, i, j);
+      }
+      continue;
+    }
+    const double d = (i == j) ? 1.0 : 0.0;
+    double x = 0.0, z = 0.0;
+    if (phase == 0) {
+      if (L.is_complex) {
+        const double* Yb = Yin + (long long)e * n * n * 2;
+        x = 0.5 * (Yb[2 * ((long long)i * n + j)] + Yb[2 * ((long long)j * n + i)]);
+        z = 0.5 * (Yb[2 * ((long long)i * n + j) + 1] + Yb[2 * ((long long)j * n + i) + 1]);
+      } else {
+        const double* Yb = Yin + (long long)e * n * n;
+        x = 0.5 * (Yb[(long long)i * n + j] + Yb[(long long)j * n + i]);
+      }
+    } else if (phase == 1) {
+      const double hp = sec.h[s - 1];
+      const double* Wep = sec.We + (s - 1) * sec.we_stride;
+      const double* Wmp = sec.Wm + (s - 1) * sec.wm_stride;
+      const double* y1p = L.y1 + ((long long)(s - 1) * L.n_energy + e) * n;
+      const double* y2p = L.y2 + ((long long)(s - 1) * L.n_energy + e) * n;
+      double sr, si;
+      get_swept(Mb, np, i, j, L.is_complex, sr, si);
+      const double ref_p = Wmp[(long long)i * n + i];
+      x = hp * (sym(Wep, n, i, j) - d * ref_p) / 3.0 + d * y1p[i] + y2p[i] * sr * y2p[j];
+      z = y2p[i] * si * y2p[j];
+    }
+    if (phase <= 1) {
+      const double ref = Wm[(long long)i * n + i];
+      x += h * (sym(Ws, n, i, j) - d * ref) / 3.0 + d * y1[i];
+      put_element(Mb, np, i, j, x, z, L.is_complex);
+    } else if (phase == 2) {
+      double sr, si;
+      get_swept(Mb, np, i, j, L.is_complex, sr, si);
+      const double q = L.Qm[(long long)s * L.npr * L.npr + (long long)i * L.npr + j];
+      x = 2.0 * q + 2.0 * d * y1[i] + y2[i] * sr * y2[j];
+      z = y2[i] * si * y2[j];
+      put_element(Mb, np, i, j, x, z, L.is_complex);
+    } else {
+      double sr, si;
+      get_swept(Mb, np, i, j, L.is_complex, sr, si);
+      const double ref = Wm[(long long)i * n + i];
+      x = h * (sym(We, n, i, j) - d * ref) / 3.0 + d * y1[i] + y2[i] * sr * y2[j];
+      z = y2[i] * si * y2[j];
+      if (L.is_complex) {
+        Yout[((long long)e * n * n + (long long)i * n + j) * 2] = x;
+        Yout[((long long)e * n * n + (long long)i * n + j) * 2 + 1] = z;
+      } else {
+        Yout[(long long)e * n * n + (long long)i * n + j] = x;
+      }
+    }
+  }
+}
+
+inline unsigned grid_for(long long work, int threads, unsigned cap = 1u << 16) {
+  long long blocks = (work + threads - 1) / threads;
+  if (blocks < 1) blocks = 1;
+  return (unsigned)(blocks > cap ? cap : blocks);
+}
+
+// Q_mid for every sector of the call (batched sweep over sectors, chunked to fit scratch).
+inline cudaError_t ldmd_qmid(const LdmdSectors& sec, LdmdLayout& L, int* status, cudaStream_t stream) {
+  const long long per = (long long)L.npr * L.npr;
+  ldmd_qmid_build_kernel<<<dim3(grid_for(per, 256, 4096), sec.n_sector), 256, 0, stream>>>(sec, L.n, L.npr, L.Qm);
+  const int chunk = (int)(L.scratch_doubles / sweep_scratch_doubles(L.npr));
+  for (int s0 = 0; s0 < sec.n_sector; s0 += chunk) {
+    const int cnt = (sec.n_sector - s0 < chunk) ? sec.n_sector - s0 : chunk;
+    cudaError_t e = sweep_sym(L.Qm + (long long)s0 * per, per, L.npr, cnt, L.scratch, status, stream);
+    if (e != cudaSuccess) return e;
+  }
+  ldmd_qmid_finish_kernel<<<dim3(grid_for(per, 256, 4096), sec.n_sector), 256, 0, stream>>>(sec, L.n, L.npr, L.Qm);
+  return cudaGetLastError();
+}
+
+// Propagate every energy through every sector of the call.  Y (device, n_energy x n x n,
+// complex interleaved when is_complex) is read at the first sector start and
+// overwritten with the log-derivative at the last sector end.
+inline cudaError_t ldmd_propagate(double* Y, const double* energies, double mu, const LdmdSectors& sec, LdmdLayout& L, int* status, cudaStream_t stream) {
+  ldmd_reference_kernel<<<grid_for((long long)sec.n_sector * L.n_energy * L.n, 256), 256, 0, stream>>>(sec, energies, mu, L.n, L.n_energy, L.y1, L.y2);
+  cudaError_t err = ldmd_qmid(sec, L, status, stream);
+  if (err != cudaSuccess) return err;
+  const long long nl = L.is_complex ? L.np / 2 : L.np;
+  const dim3 grid(grid_for(nl * nl, 256, 8192), L.n_energy);
+  const long long mstride = (long long)L.np * L.np;
+  for (int s = 0; s < sec.n_sector; ++s) {
+    ldmd_elementwise_kernel<<<grid, 256, 0, stream>>>(s == 0 ? 0 : 1, s, sec, L, Y, Y);
+    err = sweep_sym(L.M, mstride, L.np, L.n_energy, L.scratch, status, stream);
+    if (err != cudaSuccess) return err;
+    ldmd_elementwise_kernel<<<grid, 256, 0, stream>>>(2, s, sec, L, Y, Y);
+    err = sweep_sym(L.M, mstride, L.np, L.n_energy, L.scratch, status, stream);
+    if (err != cudaSuccess) return err;
+  }
+  ldmd_elementwise_kernel<<<grid, 256, 0, stream>>>(3, sec.n_sector - 1, sec, L, Y, Y);
+  return cudaGetLastError();
+}
+
+}  // namespace ticc

@@ -1,0 +1,74 @@
+"""Propagation runtime settings (reference ``src/pyticc/propagation/config.py:47-74``)."""
+
+from __future__ import annotations
+
+import re
+from dataclasses import dataclass
+from typing import Literal
+
+import numpy as np
+import torch
+from loguru import logger
+
+PropagationMode = Literal["inelastic", "capture"]
+_DEVICE_PATTERN = re.compile(r"(?:auto|cpu(?::\d+)?|gpu(?::\d+)?|cuda(?::\d+)?)")
+
+
+def normalize_device_spec(value: object) -> str:
+    """Normalise 'auto', 'gpu[:i]' / 'cuda[:i]' (and 'cpu[:i]', which is rejected at resolve time)."""
+    if not isinstance(value, str) or _DEVICE_PATTERN.fullmatch(value.strip().lower()) is None:
+        message = f"Propagation device must be 'auto', 'cpu', 'gpu', or '<platform>:<index>', but got {value!r}"
+        logger.error(message)
+        raise ValueError(message)
+    return value.strip().lower().replace("cuda", "gpu")
+
+
+def resolve_device(value: str) -> torch.device:
+    """The CUDA device for a request; a CPU request or a missing GPU raises RuntimeError
+    (this library has no CPU path)."""
+    requested = normalize_device_spec(value)
+    platform, _, index_text = requested.partition(":")
+    if platform == "cpu":
+        message = f"Propagation requested {requested!r}, but this library runs on CUDA devices only"
+        logger.error(message)
+        raise RuntimeError(message)
+    count = torch.cuda.device_count() if torch.cuda.is_available() else 0
+    index = int(index_text) if index_text else (torch.cuda.current_device() if count else 0)
+    if index >= count:
+        available = ", ".join(f"gpu:{i}" for i in range(count)) or "none"
+        message = f"Propagation requested {requested!r}, but available gpu devices are: {available}"
+        logger.error(message)
+        raise RuntimeError(message)
+    return torch.device("cuda", index)
+
+
+@dataclass(frozen=True, slots=True)
+class Propagation:
+    """mode: inner boundary condition; memory_mb: transient-memory target of the host
+    window iterator; device: 'auto' | 'gpu[:i]'; print_verbose: progress logging;
+    precision: 'fp64' (plain) or 'mixed' (closed channels swept in FP32)."""
+
+    mode: PropagationMode = "inelastic"
+    memory_mb: float = 512.0
+    device: str = "auto"
+    print_verbose: bool = False
+    precision: str = "fp64"
+
+    def __post_init__(self) -> None:
+        object.__setattr__(self, "device", normalize_device_spec(self.device))
+        if self.mode not in ("inelastic", "capture"):
+            message = f"Propagation mode must be 'inelastic' or 'capture', but got {self.mode!r}"
+            logger.error(message)
+            raise ValueError(message)
+        if not np.isfinite(self.memory_mb) or self.memory_mb <= 0.0:
+            message = f"Propagation memory_mb must be positive, but got {self.memory_mb}"
+            logger.error(message)
+            raise ValueError(message)
+        if not isinstance(self.print_verbose, bool):
+            message = f"Propagation print_verbose must be a boolean, but got {self.print_verbose!r}"
+            logger.error(message)
+            raise ValueError(message)
+        if self.precision not in ("fp64", "mixed"):
+            message = f"Propagation precision must be 'fp64' or 'mixed', but got {self.precision!r}"
+            logger.error(message)
+            raise ValueError(message)

@@ -1,0 +1,116 @@
+"""Windowed radial driver on the GPU (reference ``src/pyticc/propagation/runner.py:112-322``).
+
+Per window of sectors: W_base at every start/mid/end point is built on the device by the
+fused contraction (``ticc_contract`` with the U/R^2 + 2 mu [V + E_int] epilogue) straight
+from the device-resident PES grid, then ``ticc_ldmd_propagate`` advances all energies.
+Y stays on the device for the whole traversal.  Windows are sized by device memory
+(W points plus per-sector Q_mid), not by the reference's host transient-memory model.
+"""
+
+from __future__ import annotations
+
+from collections.abc import Sequence
+from math import ceil
+from time import perf_counter
+
+import numpy as np
+import torch
+from loguru import logger
+
+from .. import _native as nat
+from ..energy import get_Etot
+from ..matrix.interaction import contract_rows, device_rows
+from .config import Propagation, resolve_device
+from .grid import MAX_SECTORS_PER_WINDOW, RadialSector, radial_points_of
+from .logd import propagate_device
+
+WINDOW_BYTES = 6 * 1024**3  # device budget for one window's W points and Q_mid
+
+
+def device_window(n_channel: int, n_sector: int) -> int:
+    """Sectors per window so that (2w+1) W points + w Q_mid fit the window budget."""
+    padded = -(-n_channel // 128) * 128
+    per_sector = 8 * (2 * n_channel * n_channel + padded * padded)
+    return max(1, min(n_sector, MAX_SECTORS_PER_WINDOW, WINDOW_BYTES // per_sector))
+
+
+class DeviceHamiltonian:
+    """Device-resident pieces of one channel block: rows, U, E_int and the PES grid."""
+
+    def __init__(self, hamiltonian, device: torch.device) -> None:
+        self.rows = device_rows(hamiltonian.V_basis, device)
+        self.U = torch.as_tensor(np.ascontiguousarray(hamiltonian.U), device=device)
+        self.E_int = torch.as_tensor(np.ascontiguousarray(hamiltonian.E_int), device=device)
+        self.values = hamiltonian.potential_grid.device_values(device)
+        self.grid = hamiltonian.potential_grid
+        self.reduced_mass = hamiltonian.reduced_mass
+        self.n = hamiltonian.basis.n_channel
+
+    def W_base(self, radial_points: np.ndarray, out: torch.Tensor | None = None) -> torch.Tensor:
+        dev = self.U.device
+        index = torch.as_tensor(self.grid.selection(radial_points), device=dev)
+        potential = self.values.index_select(0, index)
+        R = torch.as_tensor(np.ascontiguousarray(radial_points), device=dev)
+        return contract_rows(self.rows, potential, radial_points=R, U=self.U, E_int=self.E_int, reduced_mass=self.reduced_mass, out=out)
+
+
+_DEVICE_HAMILTONIANS: dict[tuple[int, int], DeviceHamiltonian] = {}
+
+
+def device_hamiltonian(hamiltonian, device: torch.device) -> DeviceHamiltonian:
+    key = (id(hamiltonian), device.index)
+    cached = _DEVICE_HAMILTONIANS.get(key)
+    if cached is None:
+        cached = DeviceHamiltonian(hamiltonian, device)
+        _DEVICE_HAMILTONIANS[key] = cached
+    return cached
+
+
+def initial_logD(W0: torch.Tensor, energies: torch.Tensor, reduced_mass: float, mode: str) -> torch.Tensor:
+    """Y(R0) from diag W(R0; E) = diag W_base(R0) - 2 mu E (logd.py:48-91)."""
+    d = torch.diagonal(W0)[None, :] - 2.0 * reduced_mass * energies[:, None]
+    if mode == "inelastic":
+        return torch.diag_embed(torch.sqrt(torch.abs(d))).contiguous()
+    values = torch.where(d >= 0.0, torch.sqrt(torch.clamp(d, min=0.0)).to(torch.complex128), -1j * torch.sqrt(torch.clamp(-d, min=0.0)).to(torch.complex128))
+    return torch.diag_embed(values).contiguous()
+
+
+def propagate(hamiltonian, Etot, radial_sectors: Sequence[RadialSector], config: Propagation, *, Y_initial: torch.Tensor | None = None) -> torch.Tensor:
+    """Y at the last sector end for every energy, on the device (runner.py:112-161)."""
+    energies_np = get_Etot(Etot)
+    dev = resolve_device(config.device)
+    if not radial_sectors:
+        message = "Propagation produced no radial windows"
+        logger.error(message)
+        raise RuntimeError(message)
+    dh = device_hamiltonian(hamiltonian, dev)
+    n = dh.n
+    energies = torch.as_tensor(np.asarray(energies_np), device=dev)
+    n_sector = len(radial_sectors)
+    size = device_window(n, n_sector)
+    precision = nat.PRECISION_MIXED if config.precision == "mixed" else nat.PRECISION_FP64
+    logger.info(f"Propagation device: gpu:{dev.index}, x64=True")
+    if config.print_verbose:
+        logger.info(f"Propagation started: blocks=1, sectors={n_sector}, channels={n}, energies={energies_np.size}, pes_prefetch=False")
+    started = perf_counter()
+    interval = max(1, ceil(n_sector / 10))
+    next_report = interval
+    Y = Y_initial
+    W = torch.empty((2 * size + 1, n, n), dtype=torch.float64, device=dev)
+    done = 0
+    for s0 in range(0, n_sector, size):
+        window = tuple(radial_sectors[s0 : s0 + size])
+        points = radial_points_of(window)
+        Wv = dh.W_base(points, out=W[: points.size])
+        if Y is None:
+            Y = initial_logD(Wv[0], energies, dh.reduced_mass, config.mode)
+        halves = torch.as_tensor(np.asarray([s.radial_half_step for s in window]), device=dev)
+        stride = 2 * n * n
+        propagate_device(Y, energies, dh.reduced_mass, halves, Wv[0::2], Wv[1::2], Wv[2::2], stride=(stride, stride, stride), precision=precision)
+        done += len(window)
+        if config.print_verbose and (done == n_sector or done >= next_report):
+            torch.cuda.synchronize(dev)
+            logger.info(f"Propagation: {done}/{n_sector} sectors, R={window[-1].radial_end:.6f} bohr, wall={perf_counter() - started:.3f} s")
+            while next_report <= done:
+                next_report += interval
+    return Y

@@ -1,0 +1,140 @@
+"""Synthetic scattering systems with the shapes of the benchmark configurations.
+
+No public dataset is involved: each workload is an analytic PES on a model monomer,
+built from parameters (and a NumPy seed) so that tests and the benchmark construct
+identical inputs.  The same parameter sets, at reduced sizes, produced the committed
+golden fixtures through the reference's own API.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .basis import AtomSpec, DiatomBasis, RovibBasis, build_RovibDVR, build_SineDVR, clebsch_gordan, norm_YjK
+from .constants import AMU2AU, CM2AU, K2AU
+from .pes import PESWrapper
+from .scattering import PotentialGrid, prepare_potential
+from .system import ScattSystem, build_ScattSystem
+
+
+def rigid_rotor(B_cm: float, jmax: int) -> DiatomBasis:
+    """Rigid rotor as a one-point rovibrational basis: E_j = B j(j+1), WF = 1."""
+    j = np.arange(jmax + 1)
+    rovib = RovibBasis(grids=np.array([1.5]), E_vj=(B_cm * CM2AU * j * (j + 1.0))[None, :], WF_vj=np.ones((1, 1, jmax + 1)))
+    return DiatomBasis(rovib=rovib, energy_zero=0.0)
+
+
+def morse_diatom(De_cm: float, re: float, a: float, mass_amu: float, r_interval, n_dvr: int, vmax: int, jmax: int) -> DiatomBasis:
+    """Morse oscillator in a sine DVR; thresholds relative to (v=0, j=0)."""
+    mass = mass_amu * AMU2AU
+
+    def morse(r):
+        return De_cm * CM2AU * (1.0 - np.exp(-a * (r - re))) ** 2
+
+    rovib = build_RovibDVR(build_SineDVR(r_interval[0], r_interval[1], n_dvr, mass, morse), vmax, jmax, mass)
+    return DiatomBasis(rovib=rovib, energy_zero=float(rovib.E_vj[0, 0]))
+
+
+def lj_aniso_pes(eps_cm: float, Rm: float, a1: float, a2: float, c1: float = 0.0, c2: float = 0.0, re: float = 1.4) -> PESWrapper:
+    """V = eps[(Rm/R)^12 - 2(Rm/R)^6] (1 + a1(r) P1(cos t) + a2(r) P2(cos t)), a_k(r) = a_k (1 + c_k (r - re))."""
+
+    def interaction(R, coordinates):
+        r, theta = coordinates
+        x = np.cos(theta)
+        radial = eps_cm * CM2AU * ((Rm / R) ** 12 - 2.0 * (Rm / R) ** 6)
+        return radial * (1.0 + a1 * (1.0 + c1 * (r - re)) * x + a2 * (1.0 + c2 * (r - re)) * 0.5 * (3.0 * x * x - 1.0))
+
+    return PESWrapper(interaction=interaction)
+
+
+def bispherical_pes(terms, strength_cm: float, lj_eps_cm: float, lj_Rm: float) -> PESWrapper:
+    """sum_(l1,l2,l) c strength exp(-0.8 (R-6)) A_{l1 l2 l}(t1, t2, phi) + LJ(eps, Rm), with
+    A = sum_m <l1 m l2 -m | l 0> Ybar_{l1 m}(t1) Ybar_{l2 -m}(t2) cos(m phi)."""
+
+    def interaction(R, coordinates):
+        _, _, t1, t2, phi = coordinates
+        x1, x2 = np.cos(t1), np.cos(t2)
+        total = np.zeros_like(x1)
+        for l1, l2, lam, c in terms:
+            angular = np.zeros_like(x1)
+            for m in range(-min(l1, l2), min(l1, l2) + 1):
+                angular += clebsch_gordan(l1, m, l2, -m, lam) * norm_YjK(l1, m, x1) * norm_YjK(l2, -m, x2) * np.cos(m * phi)
+            total += c * angular
+        lj = lj_eps_cm * CM2AU * ((lj_Rm / R) ** 12 - 2.0 * (lj_Rm / R) ** 6)
+        return strength_cm * CM2AU * np.exp(-0.8 * (R - 6.0)) * total + lj
+
+    return PESWrapper(interaction=interaction)
+
+
+def bispherical_terms(lmax: int, seed: int) -> list[tuple[int, int, int, float]]:
+    rng = np.random.default_rng(seed)
+    terms = []
+    for l1 in range(lmax + 1):
+        for l2 in range(lmax + 1):
+            for lam in range(abs(l1 - l2), min(l1 + l2, lmax) + 1):
+                if (l1 + l2 + lam) % 2 == 0 and (l1, l2, lam) != (0, 0, 0):
+                    terms.append((l1, l2, lam, float(rng.normal())))
+    return terms
+
+
+def capture_pes(C6: float, wall_cm: float, seed: int) -> PESWrapper:
+    """-C6/R^6 (1 + 0.1 P2) plus a seeded anisotropic Gaussian wall exp(-((R-7)/1.5)^2) sum_k g_k P_k."""
+    g = np.random.default_rng(seed).uniform(0.2, 1.0, size=3)
+
+    def interaction(R, coordinates):
+        _, theta = coordinates
+        x = np.cos(theta)
+        p2 = 0.5 * (3.0 * x * x - 1.0)
+        wall = wall_cm * CM2AU * np.exp(-(((R - 7.0) / 1.5) ** 2)) * (g[0] + g[1] * x + g[2] * p2)
+        return -C6 / R**6 * (1.0 + 0.1 * p2) + wall
+
+    return PESWrapper(interaction=interaction)
+
+
+@dataclass
+class Workload:
+    """One (J, parity) block: system, PES grid and energies (hartree)."""
+
+    name: str
+    system: ScattSystem
+    grid: PotentialGrid
+    energies: np.ndarray
+    mode: str = "inelastic"
+
+
+def rigid_atom_diatom(*, B_cm=20.0, jmax=20, J=20, parity=1, mu_amu=18.0, eps_cm=150.0, Rm=6.5, a1=0.3, a2=0.2, n_theta=24, boundaries=(2.5, 30.0), half_steps=(0.05,), energies_cm=None, n_energy=16) -> Workload:
+    """Plain A+BC rigid rotor (the CPU-runnable configuration at full size)."""
+    energies = np.linspace(10.0, 500.0, n_energy) * CM2AU if energies_cm is None else np.asarray(energies_cm) * CM2AU
+    system = build_ScattSystem(AtomSpec(), rigid_rotor(B_cm, jmax), Jtot=J, system_parity=parity, potential=lj_aniso_pes(eps_cm, Rm, a1, a2), reduced_mass=mu_amu * AMU2AU)
+    return Workload("rigid_atom_diatom", system, prepare_potential(system, boundaries, half_steps, n_theta=n_theta), energies)
+
+
+MORSE_DEFAULTS = dict(De_cm=40000.0, re=1.4, a=1.2, mass_amu=1.0, r_interval=(0.5, 3.5), n_dvr=32, vmax=3, jmax=30)
+
+
+def morse_atom_diatom(*, J=30, parity=1, mu_amu=18.0, eps_cm=150.0, Rm=6.5, a1=0.3, a2=0.2, seed=2024, n_theta=32, boundaries=(2.5, 40.0), half_steps=(0.02,), energies_cm=None, n_energy=256, diatom=None, **diatom_args) -> Workload:
+    """Vibrating A+BC: Morse diatom (v <= 3, j <= 30) with r-dependent anisotropy c_k ~ U(-1/2, 1/2)."""
+    params = {**MORSE_DEFAULTS, **diatom_args}
+    c1, c2 = np.random.default_rng(seed).uniform(-0.5, 0.5, size=2)
+    diatom = morse_diatom(**params) if diatom is None else diatom
+    energies = np.linspace(100.0, 3000.0, n_energy) * CM2AU if energies_cm is None else np.asarray(energies_cm) * CM2AU
+    system = build_ScattSystem(AtomSpec(), diatom, Jtot=J, system_parity=parity, potential=lj_aniso_pes(eps_cm, Rm, a1, a2, c1, c2, params["re"]), reduced_mass=mu_amu * AMU2AU)
+    return Workload("morse_atom_diatom", system, prepare_potential(system, boundaries, half_steps, n_theta=n_theta), energies)
+
+
+def rotor_pair(*, B1_cm=60.0, B2_cm=2.0, jmax=8, J=6, parity=1, mu_amu=3.6, lmax=4, seed=11, strength_cm=40.0, lj_eps_cm=100.0, lj_Rm=6.0, n_theta_X=15, n_theta_Y=15, n_phi=12, boundaries=(2.5, 30.0), half_steps=(0.05,), energies_cm=None, n_energy=128) -> Workload:
+    """AB+CD rigid rotors with a seeded bispherical expansion plus isotropic LJ."""
+    terms = bispherical_terms(lmax, seed)
+    energies = np.linspace(5.0, 800.0, n_energy) * CM2AU if energies_cm is None else np.asarray(energies_cm) * CM2AU
+    system = build_ScattSystem(rigid_rotor(B1_cm, jmax), rigid_rotor(B2_cm, jmax), Jtot=J, system_parity=parity, potential=bispherical_pes(terms, strength_cm, lj_eps_cm, lj_Rm), reduced_mass=mu_amu * AMU2AU)
+    grid = prepare_potential(system, boundaries, half_steps, n_theta_X=n_theta_X, n_theta_Y=n_theta_Y, n_phi=n_phi)
+    return Workload("rotor_pair", system, grid, energies)
+
+
+def ultracold_capture(*, B_cm=0.03, jmax=40, J=10, parity=1, mu_amu=100.0, C6=1.0e4, wall_cm=500.0, seed=3, n_theta=48, boundaries=(8.0, 1500.0), half_steps=(0.05,), energies_K=None, n_energy=512) -> Workload:
+    """Capture-mode A+BC: ultracold energies log-uniform over 1 uK .. 1 mK."""
+    energies = np.geomspace(1.0e-6, 1.0e-3, n_energy) * K2AU if energies_K is None else np.asarray(energies_K) * K2AU
+    system = build_ScattSystem(AtomSpec(), rigid_rotor(B_cm, jmax), Jtot=J, system_parity=parity, potential=capture_pes(C6, wall_cm, seed), reduced_mass=mu_amu * AMU2AU)
+    return Workload("ultracold_capture", system, prepare_potential(system, boundaries, half_steps, n_theta=n_theta), energies, mode="capture")
