@@ -1,0 +1,342 @@
+"""Benchmark: S-matrix solves/s for the vibrating A+BC coupled-channel workload.
+
+Workload (synthetic, built by ``pyticc_b200.workloads.morse_atom_diatom``): Morse diatom
+(De = 40000 cm^-1, re = 1.4, a = 1.2) in a 32-point sine DVR, v <= 3, j <= 30, J = 30, both
+parities (N = 1984 / 1860 channels), cfg0-form PES with seeded r-dependent anisotropy,
+32-point theta quadrature, LDMD from 2.5 to 40 bohr at h = 0.02 (938 sectors), 256 energies
+uniform over 100-3000 cm^-1.  One step = one parity block x one batch of energies,
+propagated through every sector and matched: it yields `batch` S matrices.  Steps cycle
+over (parity, energy batch); every rank of a multi-GPU run owns different batches (weak
+scaling, no collective on the data path).
+
+Output: one JSON line on rank 0 (see the repository's benchmark contract).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "S-matrix solves/s on 1 B200: mixed+learned vs plain FP64 LogD at max|dS|<=1e-6"
+WORKLOAD = "vibrating A+BC exact CC: Morse diatom v<=3 j<=30, J=30, both parities (N=1984/1860), 938 LDMD sectors 2.5-40 bohr h=0.02, 256 energies 100-3000 cm^-1"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["native", "reference"], default="native")
+    p.add_argument("--batch", type=int, default=8, help="energies per step")
+    p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    p.add_argument("--sectors", type=int, default=0, help="limit sectors (0 = all 938); for quick checks only")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    QUERY = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [line for line in out.splitlines() if line.strip()]
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "lines", []):
+            parts = [x.strip() for x in line.split(",")]
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except (ValueError, IndexError):
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_workload(args):
+    from pyticc_b200 import workloads
+
+    halves = (0.02,)
+    bounds = (2.5, 40.0)
+    blocks = []
+    diatom = workloads.morse_diatom(**workloads.MORSE_DEFAULTS)
+    for parity in (1, -1):
+        wl = workloads.morse_atom_diatom(parity=parity, diatom=diatom, boundaries=bounds, half_steps=halves, n_energy=256)
+        blocks.append(wl)
+    return blocks
+
+
+def units(blocks, batch, rank, world, count):
+    """(block index, energy slice) for this rank's `count` steps."""
+    per_block = 256 // batch
+    total = 2 * per_block
+    out = []
+    for k in range(count):
+        u = (rank + world * k) % total
+        out.append((u // per_block, slice((u % per_block) * batch, (u % per_block + 1) * batch)))
+    return out
+
+
+def fp64_peak_tflops(torch, dev) -> float:
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn_like(a)
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 0.0
+    for _ in range(5):
+        s.record()
+        a @ b
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * 8192**3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def cpu_baseline(block, batch_energies, sample_sectors: int = 6) -> dict:
+    """Oracle (NumPy/LAPACK port of the reference) on a bounded sample: one energy through
+    `sample_sectors` sectors, extrapolated linearly to all sectors and energies."""
+    import torch
+
+    from oracle import contraction, ldmd
+    from pyticc_b200 import scattering
+
+    wl = block
+    ham = scattering.hamiltonian_for(wl.system, wl.grid)
+    n = wl.system.basis.n_channel
+    U = ham.U
+    pts = 2 * sample_sectors + 1
+    V = contraction.contract(ham.V_basis.channel_indices, ham.V_basis.B_real, None, 1.0, wl.grid.values.reshape(wl.grid.radial_points.size, -1)[:pts], n)
+    W = contraction.assemble_W_base(wl.grid.radial_points[:pts], U, wl.system.basis.E_int, wl.system.reduced_mass, V)
+    hs = np.asarray([s.radial_half_step for s in wl.grid.sectors[:sample_sectors]])
+    E = np.asarray(batch_energies[:1])
+    Y0 = ldmd.initialize_inelastic(W[0][None] - 2 * wl.system.reduced_mass * E[:, None, None] * np.eye(n))
+    t0 = time.perf_counter()
+    ldmd.propagate_logD(Y0, E, wl.system.reduced_mass, hs, W[0:-1:2], W[1::2], W[2::2])
+    elapsed = time.perf_counter() - t0
+    per_sector = elapsed / sample_sectors
+    n_sector = len(wl.grid.sectors)
+    solves_per_s = 1.0 / (per_sector * n_sector)
+    return {
+        "value": solves_per_s,
+        "unit": "solves/s",
+        "cores": torch.get_num_threads(),
+        "kind": "port",
+        "sample": f"1 energy x {sample_sectors} of {n_sector} sectors at N={n} ({elapsed:.1f} s), extrapolated linearly in sectors; NumPy/LAPACK LDMD restatement of the reference",
+    }
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import torch
+
+    torch.set_num_threads(os.cpu_count() or 1)
+    blocks = build_workload(args)
+    steps = []
+    for k in range(args.warmup + args.steps):
+        b = k % 2
+        base = cpu_baseline(blocks[b], blocks[b].energies, sample_sectors=3)
+        if k >= args.warmup:
+            steps.append(base["value"])
+    value = statistics.mean(steps)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "solves/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 / value,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "batch": 1, "precision": "fp64"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": torch.get_num_threads(), "kind": "port", "sample": "per step: 1 energy x 3 sectors of 938 at N=1984/1860, extrapolated linearly in sectors"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+
+    import pyticc_b200 as tb
+    from pyticc_b200 import _native as nat
+    from pyticc_b200 import scattering
+    from pyticc_b200.propagation import runner
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    group = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+        group = dist
+    lib = nat.load_library()
+    blocks = build_workload(args)
+    sectors_of = [b.grid.sectors if args.sectors == 0 else b.grid.sectors[: args.sectors] for b in blocks]
+    config = tb.Propagation(precision=args.precision)
+    n_total = args.warmup + args.steps
+    plan = units(blocks, args.batch, rank, world, n_total)
+
+    def one_step(block_index, energy_slice, timing_list=None):
+        wl = blocks[block_index]
+        ham = scattering.hamiltonian_for(wl.system, wl.grid)
+        energies = wl.energies[energy_slice]
+        Y = runner.propagate(ham, energies, sectors_of[block_index], config, window_timing=timing_list)
+        B, L = tb.get_Bmat_BF_to_SF(wl.system.basis)
+        Y_sf = tb.match.asymptotic.transform_device(Y, nat.as_device(B, dev, torch.float64))
+        S, n_open = tb.match.smatrix.get_Smat_device(Y_sf, sectors_of[block_index][-1].radial_end, energies, ham.reduced_mass, wl.system.basis.E_int, L)
+        return S
+
+    # warm-up (also builds and caches the Hamiltonian rows and device PES grids)
+    for k in range(args.warmup):
+        one_step(*plan[k])
+    torch.cuda.synchronize()
+    launches0 = lib.ticc_kernel_launches()
+    windows: list = []
+    if group:
+        group.barrier()
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record()
+        for k in range(args.warmup, n_total):
+            one_step(*plan[k], timing_list=windows)
+        stop.record()
+        torch.cuda.synchronize()
+    if group:
+        group.barrier()
+    launches = lib.ticc_kernel_launches() - launches0
+    elapsed = start.elapsed_time(stop) * 1e-3
+    t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
+    if group:
+        group.all_reduce(t, op=group.ReduceOp.MAX)
+    elapsed = float(t.item())
+    solves = args.steps * args.batch * world
+    value = solves / elapsed
+
+    # roofline: the LDMD propagate launches (window x energy batch), two symmetric
+    # N x N inversions (N^3 flops each) per (sector, energy)
+    prop_seconds = sum(a.elapsed_time(b) * 1e-3 for a, b, _ in windows)
+    prop_flops = sum(f for _, _, f in windows)
+    peak = fp64_peak_tflops(torch, dev) if rank == 0 else 0.0
+
+    # end-to-end through the public API: host energies in, host S and Y out, fresh device PES copy
+    e2e_value = None
+    h2d = d2h = 0
+    if rank == 0:
+        wl = blocks[plan[args.warmup][0]]
+        energies = np.ascontiguousarray(wl.energies[plan[args.warmup][1]])
+        wl.grid._device_cache.clear()
+        runner._DEVICE_HAMILTONIANS.clear()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        result = tb.solve(wl.system, energies, wl.grid, config, sectors=sectors_of[plan[args.warmup][0]])
+        e2e_seconds = time.perf_counter() - t0
+        e2e_value = len(energies) / e2e_seconds
+        h2d = int(energies.nbytes + wl.grid.values.nbytes)
+        d2h = int(result.Y_propagated.nbytes + sum(s.nbytes for s in result.Smat))
+        cpu = cpu_baseline(wl, energies)
+    if group:
+        group.barrier()
+        group.destroy_process_group()
+    if rank != 0:
+        return
+    n_channel = blocks[0].system.basis.n_channel
+    achieved = prop_flops / prop_seconds / 1e12 if prop_seconds else None
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": elapsed / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {
+            "workload": WORKLOAD,
+            "batch": args.batch,
+            "precision": args.precision,
+            "schedule": "fixed h=0.02" if args.sectors == 0 else f"first {args.sectors} sectors",
+            "l2": "inputs larger than L2 (per-energy work matrices 32 MiB each, W windows > 1 GiB)",
+        },
+        "roofline": {
+            "bound": "tensor",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "TFLOP/s",
+            "frac": achieved / peak if achieved and peak else None,
+            "traffic": None,
+            "kernel": "ticc_ldmd_propagate (batched symmetric sweeps on FP64 DMMA); peak = cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)",
+            "flops_per_unit": f"2 N^3 per (sector, energy), N={n_channel}",
+        },
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -46,6 +46,10 @@ enum { TICC_PRECISION_FP64 = 0, TICC_PRECISION_MIXED = 1 };
 /* Library ABI version (major * 10000 + minor * 100 + patch). */
 int ticc_version(void);
 
+/* Number of kernels this library has enqueued since the process loaded it (host-side
+ * counter; a diagnostic for benchmarks, not a device query).  No reference counterpart. */
+long long ticc_kernel_launches(void);
+
 /* Copy the calling thread's most recent error message into buf (NUL-terminated).
  * Returns the message length. */
 int ticc_last_error(char* buf, size_t len);

@@ -41,6 +41,7 @@ _PSZ = ctypes.POINTER(ctypes.c_size_t)
 
 SIGNATURES: dict[str, tuple[list, type]] = {
     "ticc_version": ([], _I),
+    "ticc_kernel_launches": ([], _LL),
     "ticc_last_error": ([ctypes.c_char_p, _SZ], _I),
     "ticc_sym_inverse_workspace_size": ([_I, _I, _I, _PSZ], _I),
     "ticc_sym_inverse": ([_P, _I, _I, _I, _P, _SZ, _P, _P], _I),
@@ -117,7 +118,7 @@ def as_device(value, device: torch.device, dtype: torch.dtype) -> torch.Tensor:
     """Contiguous device tensor of the requested dtype (copies only when needed)."""
     if isinstance(value, torch.Tensor):
         return value.to(device=device, dtype=dtype).contiguous()
-    array = np.ascontiguousarray(np.asarray(value))
+    array = np.array(value, copy=True, order="C")
     if np.iscomplexobj(array) and dtype == torch.float64:
         array = array.real
     return torch.as_tensor(array, device=device, dtype=dtype).contiguous()

@@ -92,6 +92,8 @@ extern "C" {
 
 int ticc_version(void) { return 10000; }
 
+long long ticc_kernel_launches(void) { return ticc::launch_counter().load(); }
+
 int ticc_last_error(char* buf, size_t len) {
   const size_t n = strlen(g_message);
   if (buf && len) {
@@ -171,9 +173,11 @@ int ticc_sym_inverse(void* M, int n, int batch, int is_complex, void* workspace,
   const long long nl = is_complex ? np / 2 : np;
   cudaStream_t s = as_stream(stream);
   sym_load_kernel<<<dim3(ticc::grid_for(nl * nl, 256, 8192), batch), 256, 0, s>>>(static_cast<double*>(M), n, is_complex, Mw, np);
+  ticc::note_launch();
   cudaError_t e = ticc::sweep_sym(Mw, (long long)np * np, np, batch, scratch, device_status, s);
   if (e != cudaSuccess) return cuda_fail(e, "ticc_sym_inverse");
   sym_store_kernel<<<dim3(ticc::grid_for((long long)n * n, 256, 8192), batch), 256, 0, s>>>(Mw, np, static_cast<double*>(M), n, is_complex);
+  ticc::note_launch();
   e = cudaGetLastError();
   return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_sym_inverse");
 }
@@ -221,12 +225,14 @@ int ticc_contract(const double* rows_real, const double* rows_imag, const int* g
   if (n_R == 0) return TICC_OK;
   cudaStream_t s = as_stream(stream);
   ticc::contract_init_kernel<<<ticc::grid_for((long long)n_R * n_channel * n_channel, 256), 256, 0, s>>>(out, n_channel, n_R, radial_points, U, E_int, reduced_mass);
+  ticc::note_launch();
   const double scale = normalization * (U != nullptr ? 2.0 * reduced_mass : 1.0);
   for (int g = 0; g < n_groups; ++g) {
     const int rows = group_offsets[g + 1] - group_offsets[g];
     if (rows == 0) continue;
     const int t = (rows + ticc::kCTile - 1) / ticc::kCTile;
     ticc::contract_group_kernel<<<dim3(t * (t + 1) / 2, n_R), 256, 0, s>>>(rows_real, rows_imag, group_offsets[g], rows, row_out, n_grid, scale, potential, pot_stride, n_channel, out);
+    ticc::note_launch();
   }
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_contract");
@@ -259,8 +265,10 @@ int ticc_transform_bf_to_sf(const void* Y, void* Y_out, const double* B, int n, 
   cudaStream_t s = as_stream(stream);
   const long long area = (long long)np * np;
   ticc::pad_plane_kernel<<<dim3(ticc::grid_for(area, 256, 8192), 1), 256, 0, s>>>(B, n, 0, 0, Bp, np);
+  ticc::note_launch();
   for (int part = 0; part < (is_complex ? 2 : 1); ++part) {
     ticc::pad_plane_kernel<<<dim3(ticc::grid_for(area, 256, 8192), batch), 256, 0, s>>>(static_cast<const double*>(Y), n, is_complex, part, P, np);
+    ticc::note_launch();
     // T^T = (B^T Y)^T, then (B^T T^T)^T = T B = B^T Y B
     ticc::GemmBatch g1{Bp, np, 0, P, np, area, T, np, area, np, 1.0, 1};
     cudaError_t e = ticc::gemm_tn(g1, np, np, batch, s);
@@ -269,6 +277,7 @@ int ticc_transform_bf_to_sf(const void* Y, void* Y_out, const double* B, int n, 
     e = ticc::gemm_tn(g2, np, np, batch, s);
     if (e != cudaSuccess) return cuda_fail(e, "ticc_transform_bf_to_sf");
     ticc::unpad_plane_kernel<<<dim3(ticc::grid_for((long long)n * n, 256, 8192), batch), 256, 0, s>>>(P, np, static_cast<double*>(Y_out), n, is_complex, part);
+    ticc::note_launch();
   }
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_transform_bf_to_sf");
@@ -298,6 +307,7 @@ int ticc_riccati_bessel_jy(const double* ell, const double* x, int n, double* ou
   if (ell == nullptr || x == nullptr || out == nullptr || n < 0) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_riccati_bessel_jy: bad arguments");
   if (n == 0) return TICC_OK;
   riccati_kernel<<<ticc::grid_for(n, 128), 128, 0, as_stream(stream)>>>(ell, x, n, out, device_status);
+  ticc::note_launch();
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_riccati_bessel_jy");
 }
@@ -306,6 +316,7 @@ int ticc_bessel_k_logd(const double* nu, const double* x, int n, double* out, in
   if (nu == nullptr || x == nullptr || out == nullptr || n < 0) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_bessel_k_logd: bad arguments");
   if (n == 0) return TICC_OK;
   k_logd_kernel<<<ticc::grid_for(n, 128), 128, 0, as_stream(stream)>>>(nu, x, n, out, device_status);
+  ticc::note_launch();
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_bessel_k_logd");
 }

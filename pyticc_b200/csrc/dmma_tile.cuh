@@ -77,23 +77,25 @@ __device__ inline void tile_gemm_tn(TileAcc& acc, const double* A, long long lda
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt) acc.v[mt][nt][0] = acc.v[mt][nt][1] = 0.0;
 
-  double* As[2] = {smem, smem + 2 * kChunk * kStride};
-  double* Bs[2] = {smem + kChunk * kStride, smem + 3 * kChunk * kStride};
+  // stage s of the double buffer: A at smem + s * 2 * kChunk * kStride, B right after it
+  constexpr int kStage = 2 * kChunk * kStride;
   const int nchunks = K / kChunk;
-  stage_rows(As[0], A, lda, 0, tid);
-  stage_rows(Bs[0], B, ldb, 0, tid);
+  stage_rows(smem, A, lda, 0, tid);
+  stage_rows(smem + kChunk * kStride, B, ldb, 0, tid);
   cp_async_commit();
   for (int c = 0; c < nchunks; ++c) {
     if (c + 1 < nchunks) {
-      stage_rows(As[(c + 1) & 1], A, lda, (c + 1) * kChunk, tid);
-      stage_rows(Bs[(c + 1) & 1], B, ldb, (c + 1) * kChunk, tid);
+      double* next = smem + ((c + 1) & 1) * kStage;
+      stage_rows(next, A, lda, (c + 1) * kChunk, tid);
+      stage_rows(next + kChunk * kStride, B, ldb, (c + 1) * kChunk, tid);
       cp_async_commit();
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
     }
     __syncthreads();
-    mma_chunk(acc, As[c & 1], Bs[c & 1], warp, lane);
+    const double* cur = smem + (c & 1) * kStage;
+    mma_chunk(acc, cur, cur + kChunk * kStride, warp, lane);
     __syncthreads();
   }
 }

@@ -48,6 +48,7 @@ inline cudaError_t gemm_tn(const GemmBatch& g, int M, int N, int batch, cudaStre
   cudaError_t e = cudaFuncSetAttribute(gemm_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmemBytes);
   if (e != cudaSuccess) return e;
   gemm_tn_kernel<<<dim3(M / kBlock, N / kBlock, batch), kGemmThreads, kTileSmemBytes, stream>>>(g);
+  note_launch();
   return cudaGetLastError();
 }
 

@@ -217,6 +217,7 @@ inline unsigned grid_for(long long work, int threads, unsigned cap = 1u << 16) {
 inline cudaError_t ldmd_qmid(const LdmdSectors& sec, LdmdLayout& L, int* status, cudaStream_t stream) {
   const long long per = (long long)L.npr * L.npr;
   ldmd_qmid_build_kernel<<<dim3(grid_for(per, 256, 4096), sec.n_sector), 256, 0, stream>>>(sec, L.n, L.npr, L.Qm);
+  note_launch();
   const int chunk = (int)(L.scratch_doubles / sweep_scratch_doubles(L.npr));
   for (int s0 = 0; s0 < sec.n_sector; s0 += chunk) {
     const int cnt = (sec.n_sector - s0 < chunk) ? sec.n_sector - s0 : chunk;
@@ -224,6 +225,7 @@ inline cudaError_t ldmd_qmid(const LdmdSectors& sec, LdmdLayout& L, int* status,
     if (e != cudaSuccess) return e;
   }
   ldmd_qmid_finish_kernel<<<dim3(grid_for(per, 256, 4096), sec.n_sector), 256, 0, stream>>>(sec, L.n, L.npr, L.Qm);
+  note_launch();
   return cudaGetLastError();
 }
 
@@ -232,6 +234,7 @@ inline cudaError_t ldmd_qmid(const LdmdSectors& sec, LdmdLayout& L, int* status,
 // overwritten with the log-derivative at the last sector end.
 inline cudaError_t ldmd_propagate(double* Y, const double* energies, double mu, const LdmdSectors& sec, LdmdLayout& L, int* status, cudaStream_t stream) {
   ldmd_reference_kernel<<<grid_for((long long)sec.n_sector * L.n_energy * L.n, 256), 256, 0, stream>>>(sec, energies, mu, L.n, L.n_energy, L.y1, L.y2);
+  note_launch();
   cudaError_t err = ldmd_qmid(sec, L, status, stream);
   if (err != cudaSuccess) return err;
   const long long nl = L.is_complex ? L.np / 2 : L.np;
@@ -239,13 +242,16 @@ inline cudaError_t ldmd_propagate(double* Y, const double* energies, double mu, 
   const long long mstride = (long long)L.np * L.np;
   for (int s = 0; s < sec.n_sector; ++s) {
     ldmd_elementwise_kernel<<<grid, 256, 0, stream>>>(s == 0 ? 0 : 1, s, sec, L, Y, Y);
+    note_launch();
     err = sweep_sym(L.M, mstride, L.np, L.n_energy, L.scratch, status, stream);
     if (err != cudaSuccess) return err;
     ldmd_elementwise_kernel<<<grid, 256, 0, stream>>>(2, s, sec, L, Y, Y);
+    note_launch();
     err = sweep_sym(L.M, mstride, L.np, L.n_energy, L.scratch, status, stream);
     if (err != cudaSuccess) return err;
   }
   ldmd_elementwise_kernel<<<grid, 256, 0, stream>>>(3, sec.n_sector - 1, sec, L, Y, Y);
+  note_launch();
   return cudaGetLastError();
 }
 

@@ -184,19 +184,24 @@ __global__ void match_extract_kernel(MatchLayout L, const int* n_open, double* S
 inline cudaError_t match_smatrix(const double* Y, double Rmatch, const double* energies, double mu, const double* E_int, const double* Lam, double* S, int* n_open, MatchLayout& L, int* status, cudaStream_t stream) {
   const long long ne = (long long)L.n_energy * L.n;
   match_refs_kernel<<<grid_for(ne, 128), 128, 0, stream>>>(L, Rmatch, energies, mu, E_int, Lam, status);
+  note_launch();
   match_open_kernel<<<L.n_energy, 32, 0, stream>>>(L, energies, E_int, n_open, status);
+  note_launch();
   const long long nlz = L.is_complex ? L.npz / 2 : L.npz;
   match_build_z_kernel<<<dim3(grid_for(nlz * nlz, 256, 8192), L.n_energy), 256, 0, stream>>>(L, Y);
+  note_launch();
   cudaError_t err = sweep_sym(L.Z, (long long)L.npz * L.npz, L.npz, L.n_energy, L.scratch, status, stream);
   if (err != cudaSuccess) return err;
   const long long nla = L.npa / 2;
   match_build_ab_kernel<<<dim3(grid_for(nla * nla, 256, 8192), L.n_energy), 256, 0, stream>>>(L, n_open);
+  note_launch();
   err = sweep_general(L.A, (long long)L.npa * L.npa, L.npa, L.n_energy, L.scratch, status, stream);
   if (err != cudaSuccess) return err;
   GemmBatch g{L.A, L.npa, (long long)L.npa * L.npa, L.B, L.npa, (long long)L.npa * L.npa, L.C, L.npa, (long long)L.npa * L.npa, L.npa, 1.0, 0};
   err = gemm_tn(g, L.npa, L.npa, L.n_energy, stream);
   if (err != cudaSuccess) return err;
   match_extract_kernel<<<dim3(grid_for((long long)L.n * L.n, 256, 8192), L.n_energy), 256, 0, stream>>>(L, n_open, S, status);
+  note_launch();
   return cudaGetLastError();
 }
 

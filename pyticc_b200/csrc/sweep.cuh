@@ -23,112 +23,249 @@
 
 namespace ticc {
 
-constexpr int kPivotLd = kBlock + 1;
-constexpr size_t kPivotSmemBytes = size_t(kBlock) * kPivotLd * sizeof(double) + 2 * kBlock * sizeof(double) + 2 * kBlock * sizeof(int);
+constexpr int kPivotLd = kStride;  // the pivot block lives in a [128][kStride] shared tile
+constexpr int kSub = 64;           // Gauss-Jordan sub-block of the pivot block
+constexpr size_t kPivotAuxBytes = size_t(2) * kSub * kSub * sizeof(double) + 2 * kSub * sizeof(double) + 4 * sizeof(double) + (4 + kSub) * sizeof(int);
+constexpr size_t kPivotSmemBytes = size_t(kBlock) * kPivotLd * sizeof(double) + kPivotAuxBytes;
+constexpr size_t kUpdateSmemBytes = kTileSmemBytes + kPivotAuxBytes;
+
+// Gauss-Jordan exchange of a 64x64 sub-block S (row stride kPivotLd) with partial
+// pivoting over its rows, by the kPivotThreads threads of the CTA; writes the inverse in
+// natural order to X (row stride kSub).  Thread t owns column t % 64 and every 4th row
+// from t / 64, so a step updates 16 elements per thread branch-free, the pivot row and
+// column are broadcast reads and the next pivot search runs in the 4 owners of the next
+// column.  Two barriers per step.  Returns true if a pivot was zero or non-finite.
+__device__ inline bool gauss_jordan_sub(double* S, double* X, double* aux) {
+  constexpr int G = kPivotThreads / kSub;
+  constexpr int RPT = kSub / G;
+  double* prow = aux;
+  double* pcol = aux + kSub;
+  double* cand_val = aux + 2 * kSub;
+  int* cand_row = reinterpret_cast<int*>(cand_val + 4);
+  int* perm = cand_row + 4;
+  const int t = threadIdx.x, c = t & (kSub - 1), g = t / kSub;
+  unsigned used = 0u;
+  bool singular = false;
+  if (c == 0) {
+    double best = -1.0;
+    int row = kSub;
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+      const double v = fabs(S[(g + G * i) * kPivotLd]);
+      if (v > best) {
+        best = v;
+        row = g + G * i;
+      }
+    }
+    cand_val[g] = best;
+    cand_row[g] = row;
+  }
+  __syncthreads();
+  for (int j = 0; j < kSub; ++j) {
+    double best = -1.0;
+    int p = kSub;
+#pragma unroll
+    for (int q = 0; q < G; ++q) {
+      const double v = cand_val[q];
+      const int r = cand_row[q];
+      if (v > best || (v == best && r < p)) {
+        best = v;
+        p = r;
+      }
+    }
+    double a = S[p * kPivotLd + j];
+    if (!(fabs(a) > 0.0) || !isfinite(a)) {
+      singular = true;
+      a = 1.0;
+    }
+    const double inv_a = 1.0 / a;
+    if (g == 0) prow[c] = S[p * kPivotLd + c];
+    if (g == G - 1) pcol[c] = S[c * kPivotLd + j];
+    if (t == 0) perm[j] = p;
+    if (p % G == g) used |= 1u << (p / G);
+    __syncthreads();
+    const double pr = prow[c] * inv_a;
+    double pc[RPT], v[RPT];
+#pragma unroll
+    for (int u = 0; u < RPT; ++u) pc[u] = pcol[g + G * u];
+#pragma unroll
+    for (int u = 0; u < RPT; ++u) v[u] = S[(g + G * u) * kPivotLd + c];
+    const int mine = (p % G == g) ? p / G : -1;
+#pragma unroll
+    for (int u = 0; u < RPT; ++u) {
+      const double w = (c == j) ? pc[u] * inv_a : v[u] - pc[u] * pr;
+      v[u] = (u == mine) ? ((c == j) ? inv_a : -pr) : w;
+    }
+#pragma unroll
+    for (int u = 0; u < RPT; ++u) S[(g + G * u) * kPivotLd + c] = v[u];
+    if (c == j + 1) {
+      double b2 = -1.0;
+      int row = kSub;
+#pragma unroll
+      for (int u = 0; u < RPT; ++u) {
+        const double w = ((used >> u) & 1u) ? -1.0 : fabs(v[u]);
+        if (w > b2) {
+          b2 = w;
+          row = g + G * u;
+        }
+      }
+      cand_val[g] = b2;
+      cand_row[g] = row;
+    }
+    __syncthreads();
+  }
+  // inverse element (j, perm[c]) sits at exchange slot (perm[j], c)
+  int* iperm = reinterpret_cast<int*>(prow);
+  if (t < kSub) iperm[perm[t]] = t;
+  __syncthreads();
+  for (int e = t; e < kSub * kSub; e += kPivotThreads) {
+    const int jj = e / kSub, m = e % kSub;
+    X[e] = S[perm[jj] * kPivotLd + iperm[m]];
+  }
+  __syncthreads();
+  return singular;
+}
+
+// C (64x64, row stride ldc) = sign * A (64x64, lda) * B (64x64, ldb) [+ C if accumulate];
+// 256 threads, 4x4 outputs each.  No aliasing between C and A/B.
+__device__ inline void small_gemm64(double* C, int ldc, const double* A, int lda, const double* B, int ldb, double sign, bool accumulate) {
+  const int t = threadIdx.x;
+  const int i0 = (t >> 4) * 4, m0 = (t & 15) * 4;
+  double acc[4][4] = {};
+  for (int k = 0; k < kSub; ++k) {
+    double a[4], b[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) a[u] = A[(i0 + u) * lda + k];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) b[u] = B[k * ldb + m0 + u];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int w = 0; w < 4; ++w) acc[u][w] = fma(a[u], b[w], acc[u][w]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      double* d = C + (i0 + u) * ldc + m0 + w;
+      *d = accumulate ? *d + sign * acc[u][w] : sign * acc[u][w];
+    }
+  __syncthreads();
+}
+
+// Sweep the 128x128 block held in shared memory (row stride kPivotLd) in place:
+// P <- -P^{-1}, through its two 64-wide sub-blocks (the same principal pivot transform
+// as the outer sweep, one level down).  aux holds two 64x64 temporaries and the
+// Gauss-Jordan bookkeeping.
+template <bool kSym>
+__device__ inline bool sweep_block(double* P, double* aux) {
+  double* X = aux;
+  double* U = aux + kSub * kSub;
+  double* gj = aux + 2 * kSub * kSub;
+  bool singular = false;
+  for (int s = 0; s < 2; ++s) {
+    const int k0 = kSub * s, r0 = kSub * (1 - s);
+    double* Pkk = P + k0 * kPivotLd + k0;
+    double* Pkr = P + k0 * kPivotLd + r0;
+    double* Prk = P + r0 * kPivotLd + k0;
+    double* Prr = P + r0 * kPivotLd + r0;
+    singular |= gauss_jordan_sub(Pkk, X, gj);
+    small_gemm64(U, kSub, X, kSub, Pkr, kPivotLd, 1.0, false);     // U = P_KK^-1 P_KR
+    small_gemm64(Prr, kPivotLd, Prk, kPivotLd, U, kSub, -1.0, true);  // P_RR -= P_RK U
+    if (kSym) {
+      for (int e = threadIdx.x; e < kSub * kSub; e += kPivotThreads) {
+        const int i = e / kSub, m = e % kSub;
+        Pkr[i * kPivotLd + m] = U[e];
+        Prk[m * kPivotLd + i] = U[e];
+      }
+      __syncthreads();
+    } else {
+      for (int e = threadIdx.x; e < kSub * kSub; e += kPivotThreads) Pkr[(e / kSub) * kPivotLd + e % kSub] = U[e];
+      __syncthreads();
+      small_gemm64(U, kSub, Prk, kPivotLd, X, kSub, 1.0, false);     // V = P_RK P_KK^-1
+      for (int e = threadIdx.x; e < kSub * kSub; e += kPivotThreads) Prk[(e / kSub) * kPivotLd + e % kSub] = U[e];
+      __syncthreads();
+    }
+    for (int e = threadIdx.x; e < kSub * kSub; e += kPivotThreads) Pkk[(e / kSub) * kPivotLd + e % kSub] = -X[e];
+    __syncthreads();
+  }
+  return singular;
+}
+
+// Invert the pivot block of matrix b whose rows/cols start at k0; P is a [128][kStride]
+// shared tile already holding the block.  Writes -P^-1 into M_KK and P^-1 (general
+// sweep: also its transpose) into the scratch panel; the symmetric sweep symmetrises.
+template <bool kSym>
+__device__ inline void invert_pivot_block(double* P, double* aux, double* Mb, int ld, int k0, double* pinv, int b, int* status) {
+  const bool singular = sweep_block<kSym>(P, aux);
+  if (singular && threadIdx.x == 0) report_status(status, kDeviceSingularPivot, b, k0 / kBlock);
+  double* Pb = pinv + (long long)b * 2 * kBlock * kBlock;
+  for (int idx = threadIdx.x; idx < kBlock * kBlock; idx += blockDim.x) {
+    const int j = idx >> 7, m = idx & (kBlock - 1);
+    double x = -P[j * kPivotLd + m];
+    if (kSym) {
+      x = 0.5 * (x - P[m * kPivotLd + j]);
+      Pb[idx] = x;
+    } else {
+      Pb[idx] = x;
+      Pb[kBlock * kBlock + m * kBlock + j] = x;
+    }
+    Mb[(long long)(k0 + j) * ld + k0 + m] = -x;
+  }
+}
 
 template <bool kSym>
 __global__ void __launch_bounds__(kPivotThreads) sweep_pivot_kernel(double* __restrict__ M, long long mstride, int ld, int k0, double* __restrict__ pinv, int* status) {
   extern __shared__ double smem[];
   double* P = smem;
-  double* prow = P + kBlock * kPivotLd;
-  double* pcol = prow + kBlock;
-  int* used = reinterpret_cast<int*>(pcol + kBlock);
-  int* perm = used + kBlock;
-  __shared__ int s_row;
-  __shared__ double s_val;
-
+  double* aux = smem + kBlock * kPivotLd;
   const int b = blockIdx.x;
-  const int tid = threadIdx.x;
-  const int warp = tid >> 5;
-  const int lane = tid & 31;
   double* Mb = M + (long long)b * mstride;
-
-  for (int idx = tid; idx < kBlock * kBlock; idx += kPivotThreads) {
+  for (int idx = threadIdx.x; idx < kBlock * kBlock; idx += kPivotThreads) {
     const int r = idx >> 7, c = idx & (kBlock - 1);
     P[r * kPivotLd + c] = Mb[(long long)(k0 + r) * ld + k0 + c];
   }
-  if (tid < kBlock) used[tid] = 0;
   __syncthreads();
+  invert_pivot_block<kSym>(P, aux, Mb, ld, k0, pinv, b, status);
+}
 
-  bool singular = false;
-  for (int j = 0; j < kBlock; ++j) {
-    if (warp == 0) {
-      double best = -1.0;
-      int best_row = kBlock;
-      for (int r = lane; r < kBlock; r += 32) {
-        if (!used[r]) {
-          const double v = fabs(P[r * kPivotLd + j]);
-          if (v > best) {
-            best = v;
-            best_row = r;
-          }
-        }
-      }
+// Cs[r][c] += M[r0 + r][c0 + c] for a 128x128 tile; 8 global loads in flight per batch.
+__device__ inline void add_tile_from_global(double* Cs, const double* Mb, int ld, int r0, int c0) {
+  const int tid = threadIdx.x;
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const double ov = __shfl_down_sync(0xffffffffu, best, off);
-        const int orow = __shfl_down_sync(0xffffffffu, best_row, off);
-        if (ov > best || (ov == best && orow < best_row)) {
-          best = ov;
-          best_row = orow;
-        }
-      }
-      if (lane == 0) {
-        s_row = best_row;
-        used[best_row] = 1;
-        perm[j] = best_row;
-        s_val = P[best_row * kPivotLd + j];
-      }
+  for (int base = 0; base < kBlock * 64; base += 8 * kGemmThreads) {
+    double2 m[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int piece = base + u * kGemmThreads + tid;
+      m[u] = *reinterpret_cast<const double2*>(Mb + (long long)(r0 + (piece >> 6)) * ld + c0 + (piece & 63) * 2);
     }
-    __syncthreads();
-    const int p = s_row;
-    double a = s_val;
-    if (!(fabs(a) > 0.0) || !isfinite(a)) {
-      singular = true;
-      a = 1.0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int piece = base + u * kGemmThreads + tid;
+      double* d = Cs + (piece >> 6) * kStride + (piece & 63) * 2;
+      d[0] += m[u].x;
+      d[1] += m[u].y;
     }
-    if (tid < kBlock) {
-      prow[tid] = P[p * kPivotLd + tid];
-    } else if (tid < 2 * kBlock) {
-      pcol[tid - kBlock] = P[(tid - kBlock) * kPivotLd + j];
-    }
-    __syncthreads();
-    const double inv_a = 1.0 / a;
-    for (int idx = tid; idx < kBlock * kBlock; idx += kPivotThreads) {
-      const int r = idx >> 7, c = idx & (kBlock - 1);
-      double v;
-      if (r == p) {
-        v = (c == j) ? inv_a : -prow[c] * inv_a;
-      } else if (c == j) {
-        v = pcol[r] * inv_a;
-      } else {
-        v = P[r * kPivotLd + c] - pcol[r] * (prow[c] * inv_a);
-      }
-      P[r * kPivotLd + c] = v;
-    }
-    __syncthreads();
   }
-  if (singular && tid == 0) report_status(status, kDeviceSingularPivot, b, k0 / kBlock);
+}
 
-  // Inverse element (j, perm[c]) sits at exchange slot (perm[j], c).  The symmetric
-  // sweep stores the symmetrised inverse once; the general sweep stores P^-1 and
-  // its transpose (the k-major operand of the row-panel product).
-  int* iperm = used;  // reuse: iperm[perm[c]] = c
-  if (tid < kBlock) iperm[perm[tid]] = tid;
-  __syncthreads();
-  double* Pb = pinv + (long long)b * 2 * kBlock * kBlock;
-  for (int idx = tid; idx < kBlock * kBlock; idx += kPivotThreads) {
-    const int j = idx >> 7, m = idx & (kBlock - 1);
-    const double x = P[perm[j] * kPivotLd + iperm[m]];
-    if (kSym) {
-      const double y = P[perm[m] * kPivotLd + iperm[j]];
-      const double v = 0.5 * (x + y);
-      Pb[idx] = v;
-      Mb[(long long)(k0 + j) * ld + k0 + m] = -v;
-    } else {
-      Pb[idx] = x;
-      Pb[kBlock * kBlock + m * kBlock + j] = x;
-      Mb[(long long)(k0 + j) * ld + k0 + m] = -x;
+// dst[dr0 + r][dc0 + c] = src[sr0 + r][sc0 + c] for a 128x128 tile (global to global).
+__device__ inline void copy_tile(double* dst, int ldd, int dr0, int dc0, const double* src, int lds, int sr0, int sc0) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int base = 0; base < kBlock * 64; base += 8 * kGemmThreads) {
+    double2 m[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int piece = base + u * kGemmThreads + tid;
+      m[u] = *reinterpret_cast<const double2*>(src + (long long)(sr0 + (piece >> 6)) * lds + sc0 + (piece & 63) * 2);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int piece = base + u * kGemmThreads + tid;
+      *reinterpret_cast<double2*>(dst + (long long)(dr0 + (piece >> 6)) * ldd + dc0 + (piece & 63) * 2) = m[u];
     }
   }
 }
@@ -176,12 +313,7 @@ __global__ void __launch_bounds__(kGemmThreads) sweep_rowpanel_kernel(double* __
   double* Mb = M + (long long)b * mstride;
   double* Cb = cold + (long long)b * cstride;
   const int tid = threadIdx.x;
-  if (kSym) {
-    for (int piece = tid; piece < kBlock * 64; piece += kGemmThreads) {
-      const int r = piece >> 6, c = (piece & 63) * 2;
-      *reinterpret_cast<double2*>(Cb + (long long)r * ld + c0 + c) = *reinterpret_cast<const double2*>(Mb + (long long)(k0 + r) * ld + c0 + c);
-    }
-  }
+  if (kSym) copy_tile(Cb, ld, 0, c0, Mb, ld, k0, c0);
   const double* Pt = pinv + (long long)b * 2 * kBlock * kBlock + (kSym ? 0 : kBlock * kBlock);
   TileAcc acc;
   tile_gemm_tn(acc, Pt, kBlock, Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
@@ -200,12 +332,9 @@ __global__ void __launch_bounds__(kGemmThreads) sweep_colpanel_kernel(double* __
   double* Mb = M + (long long)b * mstride;
   double* Cb = cold + (long long)b * cstride;
   const int tid = threadIdx.x;
-  for (int piece = tid; piece < kBlock * 64; piece += kGemmThreads) {
-    const int r = piece >> 6, c = (piece & 63) * 2;
-    const double2 v = *reinterpret_cast<const double2*>(Mb + (long long)(r0 + r) * ld + k0 + c);
-    smem[r * kStride + c] = v.x;
-    smem[r * kStride + c + 1] = v.y;
-  }
+  for (int e = tid; e < kBlock * kBlock; e += kGemmThreads) smem[(e >> 7) * kStride + (e & (kBlock - 1))] = 0.0;
+  __syncthreads();
+  add_tile_from_global(smem, Mb, ld, r0, k0);
   __syncthreads();
   for (int piece = tid; piece < kBlock * 64; piece += kGemmThreads) {
     const int k = piece >> 6, i = (piece & 63) * 2;
@@ -231,37 +360,63 @@ __device__ __forceinline__ void lower_pair(int idx, int& a, int& b) {
 }
 
 // Trailing update M_RR -= cold^T U: the symmetric sweep visits the lower-triangular
-// tiles and mirrors them, the general sweep visits every tile.
+// tiles and mirrors them, the general sweep visits every tile.  The grid is linear:
+// its first `batch` CTAs own the next pivot block (kb+1, kb+1) of each matrix and,
+// after their tile, invert it in place while the other CTAs finish the update, so the
+// next step's row panel starts without a separate pivot launch.
 template <bool kSym>
-__global__ void __launch_bounds__(kGemmThreads) sweep_update_kernel(double* __restrict__ M, long long mstride, int ld, int kb, const double* __restrict__ cold, long long cstride, int tiles_per_dim) {
+__global__ void __launch_bounds__(kGemmThreads) sweep_update_kernel(double* __restrict__ M, long long mstride, int ld, int kb, const double* __restrict__ cold, long long cstride, int tiles_per_dim, int batch, int fuse_next, double* __restrict__ pinv, int* status) {
   extern __shared__ double smem[];
-  const int b = blockIdx.y;
-  int ta, tb;
-  if (kSym) {
-    lower_pair(blockIdx.x, ta, tb);
+  const int t = tiles_per_dim;  // tiles per dimension excluding the pivot block kb
+  const int per = kSym ? t * (t + 1) / 2 : t * t;
+  int b, ta, tb;
+  bool next_pivot = false;
+  long long idx = blockIdx.x;
+  if (fuse_next && idx < batch) {
+    b = (int)idx;
+    ta = tb = kb + 1;
+    next_pivot = true;
   } else {
-    ta = blockIdx.x / tiles_per_dim;
-    tb = blockIdx.x % tiles_per_dim;
+    if (fuse_next) idx -= batch;
+    b = (int)(idx / per);
+    int local = (int)(idx % per);
+    if (kSym) {
+      lower_pair(local, ta, tb);
+    } else {
+      ta = local / t;
+      tb = local % t;
+    }
+    ta += (ta >= kb) ? 1 : 0;
+    tb += (tb >= kb) ? 1 : 0;
+    if (fuse_next && ta == kb + 1 && tb == kb + 1) return;  // owned by a pivot CTA
   }
-  ta += (ta >= kb) ? 1 : 0;
-  tb += (tb >= kb) ? 1 : 0;
   const int r0 = ta * kBlock, c0 = tb * kBlock, k0 = kb * kBlock;
   double* Mb = M + (long long)b * mstride;
   const double* Cb = cold + (long long)b * cstride;
+  const int tid = threadIdx.x;
+  // pull this tile of M towards L2 while the product runs
+  for (int line = tid; line < kBlock * 8; line += kGemmThreads) {
+    const double* addr = Mb + (long long)(r0 + (line >> 3)) * ld + c0 + (line & 7) * 16;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(addr));
+  }
   TileAcc acc;
   tile_gemm_tn(acc, Cb + r0, ld, Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
-  // C = M_tile - acc, staged in shared memory for the (mirrored) store
-  const int tid = threadIdx.x;
   acc_to_smem(acc, smem, -1.0);
   __syncthreads();
-  for (int piece = tid; piece < kBlock * 64; piece += kGemmThreads) {
-    const int r = piece >> 6, c = (piece & 63) * 2;
-    const double2 m = *reinterpret_cast<const double2*>(Mb + (long long)(r0 + r) * ld + c0 + c);
-    smem[r * kStride + c] += m.x;
-    smem[r * kStride + c + 1] += m.y;
-  }
+  add_tile_from_global(smem, Mb, ld, r0, c0);
   __syncthreads();
-  store_tile(Mb, ld, r0, c0, smem, kSym);
+  if (!next_pivot) {
+    store_tile(Mb, ld, r0, c0, smem, kSym);
+    return;
+  }
+  if (kSym) {  // symmetrise the pivot block from its lower half, as store_tile would
+    for (int e = tid; e < kBlock * kBlock; e += kGemmThreads) {
+      const int r = e >> 7, c = e & (kBlock - 1);
+      if (r < c) smem[r * kStride + c] = smem[c * kStride + r];
+    }
+    __syncthreads();
+  }
+  invert_pivot_block<kSym>(smem, smem + kBlock * kStride, Mb, ld, r0, pinv, b, status);
 }
 
 // Scratch per matrix: cold (kBlock x np) + P^-1 and its transpose (2 x kBlock x kBlock).
@@ -273,7 +428,7 @@ inline cudaError_t sweep_configure_variant() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(sweep_rowpanel_kernel<kSym>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmemBytes);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(sweep_update_kernel<kSym>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmemBytes);
+  return cudaFuncSetAttribute(sweep_update_kernel<kSym>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmemBytes);
 }
 
 inline cudaError_t sweep_configure() {
@@ -287,6 +442,8 @@ inline cudaError_t sweep_configure() {
 
 // Sweep every block of `batch` matrices of padded size np (a multiple of kBlock):
 // M <- -M^{-1}.  scratch holds batch * sweep_scratch_doubles(np) doubles.
+// Launches: one pivot kernel, then per block a row panel (and column panel for the
+// general sweep) and an update that also inverts the next pivot block.
 template <bool kSym>
 inline cudaError_t sweep_batched(double* M, long long mstride, int np, int batch, double* scratch, int* status, cudaStream_t stream) {
   cudaError_t e = sweep_configure();
@@ -295,15 +452,20 @@ inline cudaError_t sweep_batched(double* M, long long mstride, int np, int batch
   const long long cstride = (long long)kBlock * np;
   double* cold = scratch;
   double* pinv = scratch + (long long)batch * cstride;
+  sweep_pivot_kernel<kSym><<<batch, kPivotThreads, kPivotSmemBytes, stream>>>(M, mstride, np, 0, pinv, status);
+  note_launch();
   for (int kb = 0; kb < nt; ++kb) {
-    sweep_pivot_kernel<kSym><<<batch, kPivotThreads, kPivotSmemBytes, stream>>>(M, mstride, np, kb * kBlock, pinv, status);
-    if (nt > 1) {
-      const int t = nt - 1;
-      sweep_rowpanel_kernel<kSym><<<dim3(t, batch), kGemmThreads, kTileSmemBytes, stream>>>(M, mstride, np, kb, pinv, cold, cstride);
-      if (!kSym) sweep_colpanel_kernel<<<dim3(t, batch), kGemmThreads, kTileSmemBytes, stream>>>(M, mstride, np, kb, pinv, cold, cstride);
-      const int tiles = kSym ? t * (t + 1) / 2 : t * t;
-      sweep_update_kernel<kSym><<<dim3(tiles, batch), kGemmThreads, kTileSmemBytes, stream>>>(M, mstride, np, kb, cold, cstride, t);
-    }
+    if (nt == 1) break;
+    const int t = nt - 1;
+    sweep_rowpanel_kernel<kSym><<<dim3(t, batch), kGemmThreads, kTileSmemBytes, stream>>>(M, mstride, np, kb, pinv, cold, cstride);
+    note_launch();
+    if (!kSym) sweep_colpanel_kernel<<<dim3(t, batch), kGemmThreads, kTileSmemBytes, stream>>>(M, mstride, np, kb, pinv, cold, cstride);
+    note_launch();
+    const int per = kSym ? t * (t + 1) / 2 : t * t;
+    const int fuse = (kb + 1 < nt) ? 1 : 0;
+    const long long blocks = (long long)per * batch + (fuse ? batch : 0);
+    sweep_update_kernel<kSym><<<(unsigned)blocks, kGemmThreads, kUpdateSmemBytes, stream>>>(M, mstride, np, kb, cold, cstride, t, batch, fuse, pinv, status);
+    note_launch();
   }
   return cudaGetLastError();
 }

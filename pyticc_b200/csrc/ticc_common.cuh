@@ -14,6 +14,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 
@@ -34,6 +35,13 @@ enum DeviceStatus : int {
   kDeviceBesselFailed = 3,    // a Bessel continued fraction did not converge
   kDeviceThreshold = 4,       // a total energy sits exactly on a channel threshold
 };
+
+// Host-side count of kernels this library has enqueued (process lifetime).
+inline std::atomic<long long>& launch_counter() {
+  static std::atomic<long long> count{0};
+  return count;
+}
+inline void note_launch(long long n = 1) { launch_counter().fetch_add(n, std::memory_order_relaxed); }
 
 inline __host__ __device__ long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
 

@@ -75,8 +75,11 @@ def initial_logD(W0: torch.Tensor, energies: torch.Tensor, reduced_mass: float, 
     return torch.diag_embed(values).contiguous()
 
 
-def propagate(hamiltonian, Etot, radial_sectors: Sequence[RadialSector], config: Propagation, *, Y_initial: torch.Tensor | None = None) -> torch.Tensor:
-    """Y at the last sector end for every energy, on the device (runner.py:112-161)."""
+def propagate(hamiltonian, Etot, radial_sectors: Sequence[RadialSector], config: Propagation, *, Y_initial: torch.Tensor | None = None, window_timing: list | None = None) -> torch.Tensor:
+    """Y at the last sector end for every energy, on the device (runner.py:112-161).
+
+    ``window_timing`` (optional list) receives (start event, stop event, algorithmic
+    flops) per LDMD launch: two symmetric N x N inversions (N^3 each) per (sector, energy)."""
     energies_np = get_Etot(Etot)
     dev = resolve_device(config.device)
     if not radial_sectors:
@@ -85,7 +88,7 @@ def propagate(hamiltonian, Etot, radial_sectors: Sequence[RadialSector], config:
         raise RuntimeError(message)
     dh = device_hamiltonian(hamiltonian, dev)
     n = dh.n
-    energies = torch.as_tensor(np.asarray(energies_np), device=dev)
+    energies = torch.as_tensor(np.array(energies_np), device=dev)
     n_sector = len(radial_sectors)
     size = device_window(n, n_sector)
     precision = nat.PRECISION_MIXED if config.precision == "mixed" else nat.PRECISION_FP64
@@ -106,7 +109,13 @@ def propagate(hamiltonian, Etot, radial_sectors: Sequence[RadialSector], config:
             Y = initial_logD(Wv[0], energies, dh.reduced_mass, config.mode)
         halves = torch.as_tensor(np.asarray([s.radial_half_step for s in window]), device=dev)
         stride = 2 * n * n
+        if window_timing is not None:
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record()
         propagate_device(Y, energies, dh.reduced_mass, halves, Wv[0::2], Wv[1::2], Wv[2::2], stride=(stride, stride, stride), precision=precision)
+        if window_timing is not None:
+            t1.record()
+            window_timing.append((t0, t1, 2.0 * float(n) ** 3 * len(window) * energies.numel()))
         done += len(window)
         if config.print_verbose and (done == n_sector or done >= next_report):
             torch.cuda.synchronize(dev)

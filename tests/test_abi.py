@@ -14,7 +14,7 @@ from pyticc_b200 import _native as nat
 
 def _declared_symbols() -> set[str]:
     text = nat.HEADER_PATH.read_text()
-    return set(re.findall(r"^\s*int\s+(ticc_\w+)\s*\(", text, flags=re.MULTILINE))
+    return set(re.findall(r"^\s*(?:int|long long)\s+(ticc_\w+)\s*\(", text, flags=re.MULTILINE))
 
 
 @pytest.fixture(scope="module")
