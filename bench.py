@@ -38,7 +38,7 @@ def parse_args():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["native", "reference"], default="native")
-    p.add_argument("--batch", type=int, default=8, help="energies per step")
+    p.add_argument("--batch", type=int, default=16, help="energies per step")
     p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     p.add_argument("--sectors", type=int, default=0, help="limit sectors (0 = all 938); for quick checks only")
     return p.parse_args()
