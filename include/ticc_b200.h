@@ -63,6 +63,20 @@ int ticc_last_error(char* buf, size_t len);
 int ticc_sym_inverse_workspace_size(int n, int batch, int is_complex, size_t* bytes);
 int ticc_sym_inverse(void* M, int n, int batch, int is_complex, void* workspace, size_t workspace_bytes, int* device_status, void* stream);
 
+/* Allocation-free variant of ticc_sym_inverse, for callers that cannot allocate device
+ * memory: code running while a stream is captured into a CUDA graph (no cudaMalloc
+ * there), plugin hosts that pass only buffers they own, and C/Fortran drivers without a
+ * device allocator.  It has no counterpart in the reference.  Scratch comes from a fixed
+ * 32 MiB device array inside the library (held by every GPU that loads it until the
+ * process exits), so batch * (Np^2 + 128 Np + 32768) doubles must fit in 32 MiB, with
+ * Np = n (2n when complex) rounded up to 128 — e.g. n <= 512 with batch <= 11; larger
+ * requests are rejected with TICC_ERR_INVALID_ARGUMENT and a message.  The first call on
+ * a device looks up the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  All calls on a device share
+ * the one array: calls that overlap on the GPU (different streams, or threads) race and
+ * must be serialised by the caller.  No part of the array needs clearing between calls. */
+int ticc_sym_inverse_noalloc(void* M, int n, int batch, int is_complex, int* device_status, void* stream);
+
 /* ---- LDMD propagation -------------------------------------------------------
  * Propagate n_energy log-derivative matrices Y through n_sector Manolopoulos LDMD
  * sectors.  Replaces propagate_logD (propagation/logd.py:340-398) with its

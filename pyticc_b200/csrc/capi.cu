@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "../../include/ticc_b200.h"
 #include "contract.cuh"
@@ -344,6 +345,74 @@ int ticc_match_smatrix(const void* Y, int is_complex, double Rmatch, const doubl
   match_layout(Lay, n_channel, n_energy, is_complex, max_open, static_cast<char*>(workspace));
   cudaError_t e = ticc::match_smatrix(static_cast<const double*>(Y), Rmatch, energies, reduced_mass, E_int, L, S, n_open, Lay, device_status, as_stream(stream));
   return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_match_smatrix");
+}
+
+// ---- allocation-free symmetric inversion -------------------------------------------------
+// For callers that cannot allocate device memory themselves: code that runs while a CUDA
+// stream is being captured into a graph (cudaMalloc is not allowed there), plugin hosts
+// that hand this library only the buffers they already own, and drivers written in
+// languages without a device allocator of their own (a Fortran or C program that links
+// just this ABI).  The scratch lives in a fixed array compiled into the library instead
+// of a caller workspace.
+
+}  // extern "C"
+
+namespace {
+
+// 32 MiB of scratch; every GPU that loads the library holds it until the process exits.
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
+__device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchBytes / sizeof(double)];
+
+// Device address of g_noalloc_scratch per device ordinal (host code cannot use the symbol
+// itself: on the host it names a stand-in, not device memory).
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_address[kMaxDevices] = {};
+
+}  // namespace
+
+extern "C" {
+
+int ticc_sym_inverse_noalloc(void* M, int n, int batch, int is_complex, int* device_status, void* stream) {
+  if (M == nullptr || n < 1 || batch < 1) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_sym_inverse_noalloc: M=%p n=%d batch=%d", M, n, batch);
+  double *Mw, *scratch;
+  const size_t need = sym_layout(n, batch, is_complex, &Mw, &scratch, nullptr);
+  if (need > kNoAllocScratchBytes)
+    return fail(TICC_ERR_INVALID_ARGUMENT,
+                "ticc_sym_inverse_noalloc: n=%d batch=%d is_complex=%d needs %zu bytes of scratch, but the fixed device array holds %zu bytes "
+                "(batch * (Np^2 + 128 Np + 32768) doubles with Np = n, or 2n when complex, rounded up to 128)",
+                n, batch, is_complex, need, kNoAllocScratchBytes);
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return cuda_fail(e, "ticc_sym_inverse_noalloc: cudaGetDevice");
+  if (device < 0 || device >= kMaxDevices) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_sym_inverse_noalloc: device ordinal %d beyond %d", device, kMaxDevices);
+  double* base = nullptr;
+  {
+    // first call on a device: look up the array's device address with that device current
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_address[device] == nullptr) {
+      void* address = nullptr;
+      e = cudaGetSymbolAddress(&address, g_noalloc_scratch);
+      if (e != cudaSuccess) return cuda_fail(e, "ticc_sym_inverse_noalloc: cudaGetSymbolAddress");
+      g_noalloc_address[device] = static_cast<double*>(address);
+    }
+    base = g_noalloc_address[device];
+  }
+  // every scratch region is written before it is read (the load kernel fills the whole
+  // padded work matrix, the sweep writes its panels before using them), so nothing needs
+  // clearing between calls
+  sym_layout(n, batch, is_complex, &Mw, &scratch, reinterpret_cast<char*>(base));
+  const int np = ticc::ldmd_np(n, is_complex);
+  const long long nl = is_complex ? np / 2 : np;
+  cudaStream_t s = as_stream(stream);
+  sym_load_kernel<<<dim3(ticc::grid_for(nl * nl, 256, 8192), batch), 256, 0, s>>>(static_cast<double*>(M), n, is_complex, Mw, np);
+  ticc::note_launch();
+  e = ticc::sweep_sym(Mw, (long long)np * np, np, batch, scratch, device_status, s);
+  if (e != cudaSuccess) return cuda_fail(e, "ticc_sym_inverse_noalloc");
+  sym_store_kernel<<<dim3(ticc::grid_for((long long)n * n, 256, 8192), batch), 256, 0, s>>>(Mw, np, static_cast<double*>(M), n, is_complex);
+  ticc::note_launch();
+  e = cudaGetLastError();
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_sym_inverse_noalloc");
 }
 
 }  // extern "C"
