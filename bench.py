@@ -108,14 +108,10 @@ def build_workload(args):
 
 
 def units(blocks, batch, rank, world, count):
-    """(block index, energy slice) for this rank's `count` steps."""
-    per_block = 256 // batch
-    total = 2 * per_block
-    out = []
-    for k in range(count):
-        u = (rank + world * k) % total
-        out.append((u // per_block, slice((u % per_block) * batch, (u % per_block + 1) * batch)))
-    return out
+    """(block index, energy slice) for this rank's `count` steps (disjoint across ranks)."""
+    from pyticc_b200.replicas import rank_units
+
+    return [(u.block, slice(u.start, u.stop)) for u in rank_units(len(blocks), 256, batch, rank, world, count)]
 
 
 def fp64_peak_tflops(torch, dev) -> float:
@@ -263,11 +259,9 @@ def main():
     if group:
         group.barrier()
     launches = lib.ticc_kernel_launches() - launches0
-    elapsed = start.elapsed_time(stop) * 1e-3
-    t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
-    if group:
-        group.all_reduce(t, op=group.ReduceOp.MAX)
-    elapsed = float(t.item())
+    from pyticc_b200.replicas import max_over_ranks
+
+    elapsed = max_over_ranks(start.elapsed_time(stop) * 1e-3, group)
     solves = args.steps * args.batch * world
     value = solves / elapsed
 
@@ -279,6 +273,7 @@ def main():
 
     # end-to-end through the public API: host energies in, host S and Y out, fresh device PES copy
     e2e_value = None
+    max_dS = None
     h2d = d2h = 0
     if rank == 0:
         wl = blocks[plan[args.warmup][0]]
@@ -293,6 +288,9 @@ def main():
         h2d = int(energies.nbytes + wl.grid.values.nbytes)
         d2h = int(result.Y_propagated.nbytes + sum(s.nbytes for s in result.Smat))
         cpu = cpu_baseline(wl, energies)
+        if args.precision == "mixed":
+            plain = tb.solve(wl.system, energies, wl.grid, tb.Propagation(), sectors=sectors_of[plan[args.warmup][0]])
+            max_dS = max(float(np.abs(a - b).max()) for a, b in zip(plain.Smat, result.Smat, strict=True) if a.size)
     if group:
         group.barrier()
         group.destroy_process_group()
@@ -332,6 +330,7 @@ def main():
         },
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "accuracy": {"max_dS_vs_plain_fp64": max_dS, "tolerance": 1e-6} if args.precision == "mixed" else None,
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
     }

@@ -90,7 +90,11 @@ int ticc_sym_inverse_noalloc(void* M, int n, int batch, int is_complex, int* dev
  *   W_start/W_mid/W_end device, energy-independent W_base at the sector start,
  *              midpoint and end, each n x n (symmetric) at the given element stride
  *              between consecutive sectors (e.g. 2*n*n for an interleaved point list).
- *   precision  TICC_PRECISION_FP64 (all-FP64) or TICC_PRECISION_MIXED. */
+ *   precision  TICC_PRECISION_FP64 (all-FP64) or TICC_PRECISION_MIXED: the trailing
+ *              updates of the leading sweep blocks whose channels are all closed with a
+ *              local wavenumber above 30 bohr^-1 at the batch's highest energy run as an
+ *              FP32-accurate TF32x3 product; pivots, panels, open blocks, Q_mid and the Y
+ *              recurrence stay FP64.  Order channels most-closed first to benefit. */
 int ticc_ldmd_workspace_size(int n_channel, int n_energy, int n_sector, int is_complex, int precision, size_t* bytes);
 int ticc_ldmd_propagate(void* Y, int is_complex, const double* energies, int n_energy, double reduced_mass, const double* half_steps,
                         const double* W_start, long long W_start_stride, const double* W_mid, long long W_mid_stride, const double* W_end,

@@ -44,7 +44,7 @@ struct Carver {
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
-size_t ldmd_layout(ticc::LdmdLayout& L, int n, int n_energy, int n_sector, int is_complex, char* base) {
+size_t ldmd_layout(ticc::LdmdLayout& L, int n, int n_energy, int n_sector, int is_complex, int precision, char* base) {
   Carver c{base};
   L.n = n;
   L.n_energy = n_energy;
@@ -61,6 +61,8 @@ size_t ldmd_layout(ticc::LdmdLayout& L, int n, int n_energy, int n_sector, int i
   const size_t need_s = ticc::sweep_scratch_doubles(L.npr) * (size_t)(n_sector < 8 ? n_sector : 8);
   L.scratch_doubles = need_e > need_s ? need_e : need_s;
   L.scratch = c.take<double>(L.scratch_doubles);
+  L.reduced = (precision == TICC_PRECISION_MIXED) ? c.take<int>((size_t)n_sector) : nullptr;
+  if (base == nullptr) L.reduced = nullptr;
   return c.used + 256;
 }
 
@@ -187,9 +189,9 @@ int ticc_sym_inverse(void* M, int n, int batch, int is_complex, void* workspace,
 int ticc_ldmd_workspace_size(int n_channel, int n_energy, int n_sector, int is_complex, int precision, size_t* bytes) {
   if (n_channel < 1 || n_energy < 1 || n_sector < 1 || bytes == nullptr)
     return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_ldmd_workspace_size: n_channel=%d n_energy=%d n_sector=%d", n_channel, n_energy, n_sector);
-  if (precision != TICC_PRECISION_FP64) return fail(TICC_ERR_UNSUPPORTED, "ticc_ldmd_workspace_size: precision mode %d is not available", precision);
+  if (precision != TICC_PRECISION_FP64 && precision != TICC_PRECISION_MIXED) return fail(TICC_ERR_UNSUPPORTED, "ticc_ldmd_workspace_size: precision mode %d is not available", precision);
   ticc::LdmdLayout L{};
-  *bytes = ldmd_layout(L, n_channel, n_energy, n_sector, is_complex, nullptr);
+  *bytes = ldmd_layout(L, n_channel, n_energy, n_sector, is_complex, precision, nullptr);
   return TICC_OK;
 }
 
@@ -201,11 +203,11 @@ int ticc_ldmd_propagate(void* Y, int is_complex, const double* energies, int n_e
   if (n_channel < 1 || n_energy < 1 || n_sector < 1)
     return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_ldmd_propagate: n_channel=%d n_energy=%d n_sector=%d must be positive", n_channel, n_energy, n_sector);
   if (!(reduced_mass > 0.0)) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_ldmd_propagate: reduced_mass must be positive, got %g", reduced_mass);
-  if (precision != TICC_PRECISION_FP64) return fail(TICC_ERR_UNSUPPORTED, "ticc_ldmd_propagate: precision mode %d is not available", precision);
+  if (precision != TICC_PRECISION_FP64 && precision != TICC_PRECISION_MIXED) return fail(TICC_ERR_UNSUPPORTED, "ticc_ldmd_propagate: precision mode %d is not available", precision);
   ticc::LdmdLayout L{};
-  const size_t need = ldmd_layout(L, n_channel, n_energy, n_sector, is_complex, nullptr);
+  const size_t need = ldmd_layout(L, n_channel, n_energy, n_sector, is_complex, precision, nullptr);
   if (workspace == nullptr || workspace_bytes < need) return fail(TICC_ERR_WORKSPACE, "ticc_ldmd_propagate: workspace of %zu bytes given, %zu needed", workspace_bytes, need);
-  ldmd_layout(L, n_channel, n_energy, n_sector, is_complex, static_cast<char*>(workspace));
+  ldmd_layout(L, n_channel, n_energy, n_sector, is_complex, precision, static_cast<char*>(workspace));
   ticc::LdmdSectors sec{half_steps, W_start, W_mid, W_end, W_start_stride, W_mid_stride, W_end_stride, n_sector};
   cudaError_t e = ticc::ldmd_propagate(static_cast<double*>(Y), energies, reduced_mass, sec, L, device_status, as_stream(stream));
   return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_ldmd_propagate");

@@ -118,4 +118,115 @@ __device__ __forceinline__ void acc_to_smem(const TileAcc& acc, double* Cs, doub
     }
 }
 
+// ---- FP32-accurate tile product on the TF32 tensor pipe ---------------------------------
+// The same staged FP64 operands, split on the fly as x = hi + lo with hi, lo TF32
+// (cvt.rna), and D += A_hi B_hi + A_hi B_lo + A_lo B_hi with mma.sync m16n8k8 TF32 and
+// FP32 accumulation: ~2^-21 relative per product, about 2.5x the FP64 DMMA rate on B200.
+// Warp w owns rows (w/4)*64 .. +63 and cols (w%4)*32 .. +31 as 4 x 4 m16n8 tiles.
+struct TileAcc32 {
+  float v[4][4][4];
+};
+
+__device__ __forceinline__ void split_tf32(double x, unsigned& hi, unsigned& lo) {
+  const float f = static_cast<float>(x);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(f));
+  const float r = f - __uint_as_float(hi);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+               : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ void mma_chunk_tf32x3(TileAcc32& acc, const double* As, const double* Bs, int warp, int lane) {
+  const int wm = (warp >> 2) * 64;
+  const int wn = (warp & 3) * 32;
+  const int t = lane & 3;
+  const int g = lane >> 2;
+#pragma unroll
+  for (int kk = 0; kk < kChunk; kk += 8) {
+    unsigned ah[4][4], al[4][4], bh[4][2], bl[4][2];
+    const double* a0 = As + (kk + t) * kStride + wm + g;
+    const double* a4 = As + (kk + t + 4) * kStride + wm + g;
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt) {
+      split_tf32(a0[mt * 16], ah[mt][0], al[mt][0]);
+      split_tf32(a0[mt * 16 + 8], ah[mt][1], al[mt][1]);
+      split_tf32(a4[mt * 16], ah[mt][2], al[mt][2]);
+      split_tf32(a4[mt * 16 + 8], ah[mt][3], al[mt][3]);
+    }
+    const double* b0 = Bs + (kk + t) * kStride + wn + g;
+    const double* b4 = Bs + (kk + t + 4) * kStride + wn + g;
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      split_tf32(b0[nt * 8], bh[nt][0], bl[nt][0]);
+      split_tf32(b4[nt * 8], bh[nt][1], bl[nt][1]);
+    }
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        mma_tf32(acc.v[mt][nt], al[mt], bh[nt][0], bh[nt][1]);
+        mma_tf32(acc.v[mt][nt], ah[mt], bl[nt][0], bl[nt][1]);
+        mma_tf32(acc.v[mt][nt], ah[mt], bh[nt][0], bh[nt][1]);
+      }
+  }
+}
+
+// acc = sum_{k < K} A[k][0..127]^T B[k][0..127] in FP32-accurate TF32x3; same staging and
+// contract as tile_gemm_tn.
+__device__ inline void tile_gemm_tn_tf32x3(TileAcc32& acc, const double* A, long long lda, const double* B, long long ldb, int K, double* smem) {
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc.v[mt][nt][q] = 0.0f;
+  constexpr int kStage = 2 * kChunk * kStride;
+  const int nchunks = K / kChunk;
+  stage_rows(smem, A, lda, 0, tid);
+  stage_rows(smem + kChunk * kStride, B, ldb, 0, tid);
+  cp_async_commit();
+  for (int c = 0; c < nchunks; ++c) {
+    if (c + 1 < nchunks) {
+      double* next = smem + ((c + 1) & 1) * kStage;
+      stage_rows(next, A, lda, (c + 1) * kChunk, tid);
+      stage_rows(next + kChunk * kStride, B, ldb, (c + 1) * kChunk, tid);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const double* cur = smem + (c & 1) * kStage;
+    mma_chunk_tf32x3(acc, cur, cur + kChunk * kStride, warp, lane);
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ void acc32_to_smem(const TileAcc32& acc, double* Cs, double scale) {
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  const int wm = (warp >> 2) * 64;
+  const int wn = (warp & 3) * 32;
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      const int row = wm + mt * 16 + g;
+      const int col = wn + nt * 8 + 2 * t;
+      Cs[row * kStride + col] = scale * acc.v[mt][nt][0];
+      Cs[row * kStride + col + 1] = scale * acc.v[mt][nt][1];
+      Cs[(row + 8) * kStride + col] = scale * acc.v[mt][nt][2];
+      Cs[(row + 8) * kStride + col + 1] = scale * acc.v[mt][nt][3];
+    }
+}
+
 }  // namespace ticc

@@ -365,7 +365,7 @@ __device__ __forceinline__ void lower_pair(int idx, int& a, int& b) {
 // after their tile, invert it in place while the other CTAs finish the update, so the
 // next step's row panel starts without a separate pivot launch.
 template <bool kSym>
-__global__ void __launch_bounds__(kGemmThreads) sweep_update_kernel(double* __restrict__ M, long long mstride, int ld, int kb, const double* __restrict__ cold, long long cstride, int tiles_per_dim, int batch, int fuse_next, double* __restrict__ pinv, int* status) {
+__global__ void __launch_bounds__(kGemmThreads) sweep_update_kernel(double* __restrict__ M, long long mstride, int ld, int kb, const double* __restrict__ cold, long long cstride, int tiles_per_dim, int batch, int fuse_next, double* __restrict__ pinv, int* status, const int* __restrict__ reduced_blocks) {
   extern __shared__ double smem[];
   const int t = tiles_per_dim;  // tiles per dimension excluding the pivot block kb
   const int per = kSym ? t * (t + 1) / 2 : t * t;
@@ -399,9 +399,17 @@ __global__ void __launch_bounds__(kGemmThreads) sweep_update_kernel(double* __re
     const double* addr = Mb + (long long)(r0 + (line >> 3)) * ld + c0 + (line & 7) * 16;
     asm volatile("prefetch.global.L2 [%0];" ::"l"(addr));
   }
-  TileAcc acc;
-  tile_gemm_tn(acc, Cb + r0, ld, Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
-  acc_to_smem(acc, smem, -1.0);
+  // the leading `*reduced_blocks` pivot blocks (channels closed beyond the threshold of the
+  // mixed-precision mode) take the FP32-accurate TF32x3 product; all others FP64 DMMA
+  if (reduced_blocks != nullptr && kb < *reduced_blocks) {
+    TileAcc32 acc;
+    tile_gemm_tn_tf32x3(acc, Cb + r0, ld, Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
+    acc32_to_smem(acc, smem, -1.0);
+  } else {
+    TileAcc acc;
+    tile_gemm_tn(acc, Cb + r0, ld, Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
+    acc_to_smem(acc, smem, -1.0);
+  }
   __syncthreads();
   add_tile_from_global(smem, Mb, ld, r0, c0);
   __syncthreads();
@@ -445,7 +453,7 @@ inline cudaError_t sweep_configure() {
 // Launches: one pivot kernel, then per block a row panel (and column panel for the
 // general sweep) and an update that also inverts the next pivot block.
 template <bool kSym>
-inline cudaError_t sweep_batched(double* M, long long mstride, int np, int batch, double* scratch, int* status, cudaStream_t stream) {
+inline cudaError_t sweep_batched(double* M, long long mstride, int np, int batch, double* scratch, int* status, cudaStream_t stream, const int* reduced_blocks = nullptr) {
   cudaError_t e = sweep_configure();
   if (e != cudaSuccess) return e;
   const int nt = np / kBlock;
@@ -464,14 +472,14 @@ inline cudaError_t sweep_batched(double* M, long long mstride, int np, int batch
     const int per = kSym ? t * (t + 1) / 2 : t * t;
     const int fuse = (kb + 1 < nt) ? 1 : 0;
     const long long blocks = (long long)per * batch + (fuse ? batch : 0);
-    sweep_update_kernel<kSym><<<(unsigned)blocks, kGemmThreads, kUpdateSmemBytes, stream>>>(M, mstride, np, kb, cold, cstride, t, batch, fuse, pinv, status);
+    sweep_update_kernel<kSym><<<(unsigned)blocks, kGemmThreads, kUpdateSmemBytes, stream>>>(M, mstride, np, kb, cold, cstride, t, batch, fuse, pinv, status, reduced_blocks);
     note_launch();
   }
   return cudaGetLastError();
 }
 
-inline cudaError_t sweep_sym(double* M, long long mstride, int np, int batch, double* scratch, int* status, cudaStream_t stream) {
-  return sweep_batched<true>(M, mstride, np, batch, scratch, status, stream);
+inline cudaError_t sweep_sym(double* M, long long mstride, int np, int batch, double* scratch, int* status, cudaStream_t stream, const int* reduced_blocks = nullptr) {
+  return sweep_batched<true>(M, mstride, np, batch, scratch, status, stream, reduced_blocks);
 }
 inline cudaError_t sweep_general(double* M, long long mstride, int np, int batch, double* scratch, int* status, cudaStream_t stream) {
   return sweep_batched<false>(M, mstride, np, batch, scratch, status, stream);

@@ -35,16 +35,33 @@ def device_window(n_channel: int, n_sector: int) -> int:
 
 
 class DeviceHamiltonian:
-    """Device-resident pieces of one channel block: rows, U, E_int and the PES grid."""
+    """Device-resident pieces of one channel block: rows, U, E_int and the PES grid.
 
-    def __init__(self, hamiltonian, device: torch.device) -> None:
+    With ``closed_first`` the channels are reordered once so that the most strongly closed
+    ones (largest W_ii at the outermost grid point) come first; the mixed-precision sweep
+    takes its reduced-precision blocks from the front of that order.  ``position[c]`` is
+    the propagated index of original channel c."""
+
+    def __init__(self, hamiltonian, device: torch.device, closed_first: bool = False) -> None:
         self.rows = device_rows(hamiltonian.V_basis, device)
-        self.U = torch.as_tensor(np.ascontiguousarray(hamiltonian.U), device=device)
-        self.E_int = torch.as_tensor(np.ascontiguousarray(hamiltonian.E_int), device=device)
+        U = np.ascontiguousarray(hamiltonian.U)
+        E_int = np.ascontiguousarray(hamiltonian.E_int)
         self.values = hamiltonian.potential_grid.device_values(device)
         self.grid = hamiltonian.potential_grid
         self.reduced_mass = hamiltonian.reduced_mass
         self.n = hamiltonian.basis.n_channel
+        self.U = torch.as_tensor(U, device=device)
+        self.E_int = torch.as_tensor(E_int, device=device)
+        self.position = None
+        if closed_first:
+            outer = self.W_base(self.grid.radial_points[-1:])[0]
+            order = np.argsort(-torch.diagonal(outer).cpu().numpy(), kind="stable")
+            position = np.empty_like(order)
+            position[order] = np.arange(order.size)
+            self.U = torch.as_tensor(np.ascontiguousarray(U[np.ix_(order, order)]), device=device)
+            self.E_int = torch.as_tensor(np.ascontiguousarray(E_int[order]), device=device)
+            self.rows.row_out = torch.as_tensor(position, device=device, dtype=torch.int32)[self.rows.row_out.long()].to(torch.int32).contiguous()
+            self.position = torch.as_tensor(position, device=device)
 
     def W_base(self, radial_points: np.ndarray, out: torch.Tensor | None = None) -> torch.Tensor:
         dev = self.U.device
@@ -54,14 +71,14 @@ class DeviceHamiltonian:
         return contract_rows(self.rows, potential, radial_points=R, U=self.U, E_int=self.E_int, reduced_mass=self.reduced_mass, out=out)
 
 
-_DEVICE_HAMILTONIANS: dict[tuple[int, int], DeviceHamiltonian] = {}
+_DEVICE_HAMILTONIANS: dict[tuple[int, int, bool], DeviceHamiltonian] = {}
 
 
-def device_hamiltonian(hamiltonian, device: torch.device) -> DeviceHamiltonian:
-    key = (id(hamiltonian), device.index)
+def device_hamiltonian(hamiltonian, device: torch.device, closed_first: bool = False) -> DeviceHamiltonian:
+    key = (id(hamiltonian), device.index, closed_first)
     cached = _DEVICE_HAMILTONIANS.get(key)
     if cached is None:
-        cached = DeviceHamiltonian(hamiltonian, device)
+        cached = DeviceHamiltonian(hamiltonian, device, closed_first)
         _DEVICE_HAMILTONIANS[key] = cached
     return cached
 
@@ -86,12 +103,15 @@ def propagate(hamiltonian, Etot, radial_sectors: Sequence[RadialSector], config:
         message = "Propagation produced no radial windows"
         logger.error(message)
         raise RuntimeError(message)
-    dh = device_hamiltonian(hamiltonian, dev)
+    mixed = config.precision == "mixed"
+    dh = device_hamiltonian(hamiltonian, dev, closed_first=mixed)
     n = dh.n
     energies = torch.as_tensor(np.array(energies_np), device=dev)
     n_sector = len(radial_sectors)
     size = device_window(n, n_sector)
-    precision = nat.PRECISION_MIXED if config.precision == "mixed" else nat.PRECISION_FP64
+    precision = nat.PRECISION_MIXED if mixed else nat.PRECISION_FP64
+    if Y_initial is not None and dh.position is not None:
+        Y_initial = Y_initial[:, dh.position.argsort()][:, :, dh.position.argsort()].contiguous()
     logger.info(f"Propagation device: gpu:{dev.index}, x64=True")
     if config.print_verbose:
         logger.info(f"Propagation started: blocks=1, sectors={n_sector}, channels={n}, energies={energies_np.size}, pes_prefetch=False")
@@ -122,4 +142,6 @@ def propagate(hamiltonian, Etot, radial_sectors: Sequence[RadialSector], config:
             logger.info(f"Propagation: {done}/{n_sector} sectors, R={window[-1].radial_end:.6f} bohr, wall={perf_counter() - started:.3f} s")
             while next_report <= done:
                 next_report += interval
+    if dh.position is not None:
+        Y = Y[:, dh.position][:, :, dh.position].contiguous()
     return Y

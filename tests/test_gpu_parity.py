@@ -232,3 +232,29 @@ def test_device_status_reports_a_singular_pivot_block():
     M = np.zeros((1, 128, 128))
     with pytest.raises(RuntimeError, match="pivot block"):
         _sym_inverse(M, False)
+
+
+MIXED_TOL = 1.0e-6
+
+
+def test_mixed_precision_matches_fp64_on_vibrating_block():
+    """v <= 3 puts channels > 4000 cm^-1 above the energies: their leading blocks take the
+    TF32x3 product.  The mixed S must stay within 1e-6 of the plain FP64 S."""
+    wl = workloads.morse_atom_diatom(J=8, jmax=12, vmax=3, n_dvr=24, n_theta=16, boundaries=(2.5, 20.0), half_steps=(0.02,), energies_cm=[150.0, 1200.0, 2900.0])
+    assert wl.system.basis.n_channel > 256
+    plain = tb.solve(wl.system, wl.energies, wl.grid, tb.Propagation())
+    mixed = tb.solve(wl.system, wl.energies, wl.grid, tb.Propagation(precision="mixed"))
+    worst = max(float(np.abs(a - b).max()) for a, b in zip(plain.Smat, mixed.Smat, strict=True) if a.size)
+    assert worst <= MIXED_TOL
+    assert worst > 0.0  # the reduced-precision blocks did run
+    assert mixed.unitarity_defect().max() < 1e-6
+
+
+@pytest.mark.parametrize("name", ["solve_rigid_p+", "solve_morse"])
+def test_mixed_precision_matches_reference(name):
+    g, p, wl = _golden_workload(name)
+    result = tb.solve(wl.system, wl.energies, wl.grid, tb.Propagation(precision="mixed"))
+    for e, s in enumerate(result.Smat):
+        n = s.shape[0]
+        if n:
+            assert np.abs(s - g["Smat"][e, :n, :n]).max() <= MIXED_TOL
