@@ -151,6 +151,38 @@ int ticc_match_smatrix(const void* Y, int is_complex, double Rmatch, const doubl
                        const double* L, int n_channel, int max_open, double* S, int* n_open, void* workspace, size_t workspace_bytes,
                        int* device_status, void* stream);
 
+/* ---- learned sector widths ------------------------------------------------------
+ * No counterpart in the reference, which propagates on the fixed grid of
+ * build_radial_sectors (propagation/grid.py:193-239) only.  A small MLP proposes, per
+ * fixed-step sector, log2 of how many aligned sectors may be merged into one; merged
+ * sectors keep their start/mid/end points on the same grid, so the PotentialGrid is
+ * unchanged.  The fixed-step propagation stays the judge of every learned schedule.
+ *
+ * Network: n_feature -> n_hidden (tanh) -> n_hidden (tanh) -> 1, FP32 parameters packed as
+ * W1[n_hidden][n_feature], b1, W2[n_hidden][n_hidden], b2, w3[n_hidden], b3. */
+int ticc_mlp_shape(int* n_feature, int* n_hidden, int* n_param);
+
+/* features[s][0..7] (FP32) of fixed-step sector s from its W_base start/mid/end matrices
+ * (same layout and strides as ticc_ldmd_propagate); two_mu_emax / two_mu_emin are 2 mu E
+ * at the highest and lowest energy of the batch.  All pointers device. */
+int ticc_step_features(const double* W_start, long long W_start_stride, const double* W_mid, long long W_mid_stride, const double* W_end,
+                       long long W_end_stride, const double* half_steps, int n_sector, int n_channel, double two_mu_emax, double two_mu_emin,
+                       float* features, void* stream);
+
+/* y[i] = MLP((x[i] - norm[0:8]) * norm[8:16]) for n samples.  All pointers device. */
+int ticc_mlp_forward(const float* params, const float* norm, const float* x, int n, float* y, void* stream);
+
+/* Gradient of the asymmetric weighted squared loss
+ *   loss = inv_weight_sum * sum_i weight[i] c_i (y_i - target[i])^2,  c_i = over_weight if
+ *   y_i > target[i] (a proposal wider than the label) else 1,
+ * into grads[n_param] and loss[1] (device), summed in a fixed order. */
+int ticc_mlp_workspace_size(int n, size_t* bytes);
+int ticc_mlp_gradient(const float* params, const float* norm, const float* x, const float* target, const float* weight, int n, float over_weight,
+                      float inv_weight_sum, float* grads, float* loss, void* workspace, size_t workspace_bytes, void* stream);
+
+/* One Adam step (step counts from 1) on params with moments[2 * n_param] = (m, v). */
+int ticc_mlp_adam(float* params, const float* grads, float* moments, int step, float lr, float beta1, float beta2, float eps, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -38,6 +38,7 @@ _D = ctypes.c_double
 _LL = ctypes.c_longlong
 _SZ = ctypes.c_size_t
 _PSZ = ctypes.POINTER(ctypes.c_size_t)
+_F = ctypes.c_float
 
 SIGNATURES: dict[str, tuple[list, type]] = {
     "ticc_version": ([], _I),
@@ -55,6 +56,12 @@ SIGNATURES: dict[str, tuple[list, type]] = {
     "ticc_bessel_k_logd": ([_P, _P, _I, _P, _P, _P], _I),
     "ticc_match_workspace_size": ([_I, _I, _I, _I, _PSZ], _I),
     "ticc_match_smatrix": ([_P, _I, _D, _P, _I, _D, _P, _P, _I, _I, _P, _P, _P, _SZ, _P, _P], _I),
+    "ticc_mlp_shape": ([ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),
+    "ticc_step_features": ([_P, _LL, _P, _LL, _P, _LL, _P, _I, _I, _D, _D, _P, _P], _I),
+    "ticc_mlp_forward": ([_P, _P, _P, _I, _P, _P], _I),
+    "ticc_mlp_workspace_size": ([_I, _PSZ], _I),
+    "ticc_mlp_gradient": ([_P, _P, _P, _P, _P, _I, _F, _F, _P, _P, _P, _SZ, _P], _I),
+    "ticc_mlp_adam": ([_P, _P, _P, _I, _F, _F, _F, _F, _P], _I),
 }
 
 _lib = None

@@ -11,6 +11,7 @@
 #include "../../include/ticc_b200.h"
 #include "contract.cuh"
 #include "gemm.cuh"
+#include "learned.cuh"
 #include "ldmd.cuh"
 #include "match.cuh"
 #include "sweep.cuh"
@@ -347,6 +348,77 @@ int ticc_match_smatrix(const void* Y, int is_complex, double Rmatch, const doubl
   match_layout(Lay, n_channel, n_energy, is_complex, max_open, static_cast<char*>(workspace));
   cudaError_t e = ticc::match_smatrix(static_cast<const double*>(Y), Rmatch, energies, reduced_mass, E_int, L, S, n_open, Lay, device_status, as_stream(stream));
   return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_match_smatrix");
+}
+
+// ---- learned sector widths -------------------------------------------------------------------------
+int ticc_mlp_shape(int* n_feature, int* n_hidden, int* n_param) {
+  if (n_feature == nullptr || n_hidden == nullptr || n_param == nullptr) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_mlp_shape: null output pointer");
+  *n_feature = ticc::kFeat;
+  *n_hidden = ticc::kHidden;
+  *n_param = ticc::kParams;
+  return TICC_OK;
+}
+
+int ticc_step_features(const double* W_start, long long W_start_stride, const double* W_mid, long long W_mid_stride, const double* W_end, long long W_end_stride,
+                       const double* half_steps, int n_sector, int n_channel, double two_mu_emax, double two_mu_emin, float* features, void* stream) {
+  if (W_start == nullptr || W_mid == nullptr || W_end == nullptr || half_steps == nullptr || features == nullptr)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_step_features: null pointer");
+  if (n_sector < 0 || n_channel < 1) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_step_features: n_sector=%d n_channel=%d", n_sector, n_channel);
+  if (n_sector == 0) return TICC_OK;
+  ticc::step_features_kernel<<<n_sector, ticc::kFeatureThreads, 0, as_stream(stream)>>>(W_start, W_start_stride, W_mid, W_mid_stride, W_end, W_end_stride, half_steps, n_channel,
+                                                                                        two_mu_emax, two_mu_emin, features);
+  ticc::note_launch();
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_step_features");
+}
+
+int ticc_mlp_forward(const float* params, const float* norm, const float* x, int n, float* y, void* stream) {
+  if (params == nullptr || norm == nullptr || x == nullptr || y == nullptr) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_mlp_forward: null pointer");
+  if (n < 0) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_mlp_forward: n=%d", n);
+  if (n == 0) return TICC_OK;
+  ticc::mlp_forward_kernel<<<(n + 127) / 128, 128, 0, as_stream(stream)>>>(params, norm, x, n, y);
+  ticc::note_launch();
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_mlp_forward");
+}
+
+int ticc_mlp_workspace_size(int n, size_t* bytes) {
+  if (n < 1 || bytes == nullptr) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_mlp_workspace_size: n=%d", n);
+  *bytes = ticc::mlp_workspace_floats(n) * sizeof(float) + 256;
+  return TICC_OK;
+}
+
+int ticc_mlp_gradient(const float* params, const float* norm, const float* x, const float* target, const float* weight, int n, float over_weight, float inv_weight_sum,
+                      float* grads, float* loss, void* workspace, size_t workspace_bytes, void* stream) {
+  if (params == nullptr || norm == nullptr || x == nullptr || target == nullptr || weight == nullptr || grads == nullptr || loss == nullptr)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_mlp_gradient: null pointer");
+  if (n < 1 || !(over_weight > 0.0f) || !(inv_weight_sum > 0.0f))
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_mlp_gradient: n=%d over_weight=%g inv_weight_sum=%g", n, over_weight, inv_weight_sum);
+  const size_t need = ticc::mlp_workspace_floats(n) * sizeof(float) + 256;
+  if (workspace == nullptr || workspace_bytes < need) return fail(TICC_ERR_WORKSPACE, "ticc_mlp_gradient: workspace of %zu bytes given, %zu needed", workspace_bytes, need);
+  Carver c{static_cast<char*>(workspace)};
+  const int nb = ticc::mlp_grad_blocks(n);
+  float* partials = c.take<float>((size_t)nb * ticc::kParams);
+  float* loss_partials = c.take<float>((size_t)nb);
+  cudaError_t e = cudaFuncSetAttribute(ticc::mlp_partial_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ticc::kMlpGradSmemBytes);
+  if (e != cudaSuccess) return cuda_fail(e, "ticc_mlp_gradient");
+  cudaStream_t s = as_stream(stream);
+  ticc::mlp_partial_grad_kernel<<<nb, ticc::kMlpSamples, ticc::kMlpGradSmemBytes, s>>>(params, norm, x, target, weight, n, over_weight, inv_weight_sum, partials, loss_partials);
+  ticc::note_launch();
+  ticc::mlp_reduce_kernel<<<(ticc::kParams + 255) / 256, 256, 0, s>>>(partials, loss_partials, nb, grads, loss);
+  ticc::note_launch();
+  e = cudaGetLastError();
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_mlp_gradient");
+}
+
+int ticc_mlp_adam(float* params, const float* grads, float* moments, int step, float lr, float beta1, float beta2, float eps, void* stream) {
+  if (params == nullptr || grads == nullptr || moments == nullptr) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_mlp_adam: null pointer");
+  if (step < 1 || !(lr > 0.0f) || !(beta1 >= 0.0f && beta1 < 1.0f) || !(beta2 >= 0.0f && beta2 < 1.0f) || !(eps > 0.0f))
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_mlp_adam: step=%d lr=%g beta1=%g beta2=%g eps=%g", step, lr, beta1, beta2, eps);
+  ticc::mlp_adam_kernel<<<(ticc::kParams + 255) / 256, 256, 0, as_stream(stream)>>>(params, grads, moments, step, lr, beta1, beta2, eps);
+  ticc::note_launch();
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_mlp_adam");
 }
 
 // ---- allocation-free symmetric inversion -------------------------------------------------

@@ -46,13 +46,18 @@ def resolve_device(value: str) -> torch.device:
 class Propagation:
     """mode: inner boundary condition; memory_mb: transient-memory target of the host
     window iterator; device: 'auto' | 'gpu[:i]'; print_verbose: progress logging;
-    precision: 'fp64' (plain) or 'mixed' (closed channels swept in FP32)."""
+    precision: 'fp64' (plain) or 'mixed' (closed channels swept in FP32);
+    steps: 'fixed' (the PotentialGrid's sectors) or 'learned' (aligned merges of them
+    proposed by ``proposer``, a StepProposer or a path to its weights; None = the
+    packaged default)."""
 
     mode: PropagationMode = "inelastic"
     memory_mb: float = 512.0
     device: str = "auto"
     print_verbose: bool = False
     precision: str = "fp64"
+    steps: str = "fixed"
+    proposer: object = None
 
     def __post_init__(self) -> None:
         object.__setattr__(self, "device", normalize_device_spec(self.device))
@@ -70,5 +75,9 @@ class Propagation:
             raise ValueError(message)
         if self.precision not in ("fp64", "mixed"):
             message = f"Propagation precision must be 'fp64' or 'mixed', but got {self.precision!r}"
+            logger.error(message)
+            raise ValueError(message)
+        if self.steps not in ("fixed", "learned"):
+            message = f"Propagation steps must be 'fixed' or 'learned', but got {self.steps!r}"
             logger.error(message)
             raise ValueError(message)

@@ -229,6 +229,10 @@ def solve(problem: ScattSystem, Etot, potential_grid: PotentialGrid, propagation
         raise ValueError(message)
     hamiltonian = hamiltonian_for(problem, potential_grid)
     run_sectors = potential_grid.sectors if sectors is None else tuple(sectors)
+    if sectors is None and propagation.steps == "learned":
+        from ..propagation.learned import learned_sectors, resolve_proposer
+
+        run_sectors = learned_sectors(hamiltonian, run_sectors, energies, resolve_proposer(propagation.proposer), propagation.device)
     Y = propagate(hamiltonian, energies, run_sectors, propagation)
     B, L = get_Bmat_BF_to_SF(basis)
     Y_sf = transform_device(Y, nat.as_device(B, Y.device, torch.float64))
