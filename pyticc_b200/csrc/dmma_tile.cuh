@@ -34,10 +34,11 @@ struct TileAcc {
   double v[8][4][2];
 };
 
-// Stage rows [k, k + kChunk) of a k-major operand (128 contiguous doubles per row).
+// Stage rows [k, k + kC) of a k-major operand (128 contiguous doubles per row).
+template <int kC = kChunk>
 __device__ __forceinline__ void stage_rows(double* dst, const double* src, long long ld, int k, int tid) {
 #pragma unroll
-  for (int i = 0; i < (kChunk * 64) / kGemmThreads; ++i) {
+  for (int i = 0; i < (kC * 64) / kGemmThreads; ++i) {
     const int piece = tid + i * kGemmThreads;
     const int r = piece >> 6;
     const int c = (piece & 63) * 2;
@@ -45,13 +46,14 @@ __device__ __forceinline__ void stage_rows(double* dst, const double* src, long 
   }
 }
 
+template <int kC = kChunk>
 __device__ __forceinline__ void mma_chunk(TileAcc& acc, const double* As, const double* Bs, int warp, int lane) {
   const int wm = (warp >> 2) * 64;
   const int wn = (warp & 3) * 32;
   const int kr = lane & 3;
   const int mr = lane >> 2;
 #pragma unroll
-  for (int kk = 0; kk < kChunk; kk += 4) {
+  for (int kk = 0; kk < kC; kk += 4) {
     double a[8], b[4];
     const double* arow = As + (kk + kr) * kStride + wm + mr;
     const double* brow = Bs + (kk + kr) * kStride + wn + mr;
@@ -140,13 +142,14 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], 
                : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+template <int kC = kChunk>
 __device__ __forceinline__ void mma_chunk_tf32x3(TileAcc32& acc, const double* As, const double* Bs, int warp, int lane) {
   const int wm = (warp >> 2) * 64;
   const int wn = (warp & 3) * 32;
   const int t = lane & 3;
   const int g = lane >> 2;
 #pragma unroll
-  for (int kk = 0; kk < kChunk; kk += 8) {
+  for (int kk = 0; kk < kC; kk += 8) {
     unsigned ah[4][4], al[4][4], bh[4][2], bl[4][2];
     const double* a0 = As + (kk + t) * kStride + wm + g;
     const double* a4 = As + (kk + t + 4) * kStride + wm + g;
@@ -227,6 +230,128 @@ __device__ __forceinline__ void acc32_to_smem(const TileAcc32& acc, double* Cs, 
       Cs[(row + 8) * kStride + col] = scale * acc.v[mt][nt][2];
       Cs[(row + 8) * kStride + col + 1] = scale * acc.v[mt][nt][3];
     }
+}
+
+// ---- trailing-update tile with the C tile staged during the product ----------------------
+// The update M_tile -= A^T B of the sweep reads the 128 x 128 FP64 tile of M once; here it
+// is copied into shared memory by cp.async while the first K-chunk is multiplied, so the
+// epilogue is an in-place shared-memory subtraction instead of a global read after the
+// product.  K-chunks of kUpdChunk rows keep both staging buffers and the C tile resident:
+//   [ A/B stages: 2 x 2 x kUpdChunk x kStride ][ C tile: 128 x kStride ]   (doubles)
+constexpr int kUpdChunk = 16;
+constexpr int kUpdStageDoubles = 2 * 2 * kUpdChunk * kStride;  // 8448 doubles = 67584 B
+constexpr size_t kUpdTileSmemBytes = (size_t(kUpdStageDoubles) + size_t(kBlock) * kStride) * sizeof(double);  // 202752
+
+__device__ __forceinline__ void mma_chunk_any(TileAcc& acc, const double* As, const double* Bs, int warp, int lane) { mma_chunk<kUpdChunk>(acc, As, Bs, warp, lane); }
+__device__ __forceinline__ void mma_chunk_any(TileAcc32& acc, const double* As, const double* Bs, int warp, int lane) { mma_chunk_tf32x3<kUpdChunk>(acc, As, Bs, warp, lane); }
+__device__ __forceinline__ void acc_zero(TileAcc& acc) {
+#pragma unroll
+  for (int mt = 0; mt < 8; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) acc.v[mt][nt][0] = acc.v[mt][nt][1] = 0.0;
+}
+__device__ __forceinline__ void acc_zero(TileAcc32& acc) {
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc.v[mt][nt][q] = 0.0f;
+}
+
+// acc = sum_{k < K} A[k][.]^T B[k][.] (K a multiple of kUpdChunk, at least 2 chunks) while
+// Cs <- C[r][c] for the 128 x 128 tile at Cg (row stride ldc).  On return Cs holds C and the
+// staging region is free (ends with a __syncthreads()).
+template <class Acc>
+__device__ inline void tile_update_product(Acc& acc, const double* A, long long lda, const double* B, long long ldb, int K, double* stages, double* Cs, const double* Cg, long long ldc) {
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  acc_zero(acc);
+  constexpr int kStage = 2 * kUpdChunk * kStride;
+  const int nchunks = K / kUpdChunk;
+  // commit groups in order: chunk 0, C tile, chunk 1, chunk 2, ...
+  stage_rows<kUpdChunk>(stages, A, lda, 0, tid);
+  stage_rows<kUpdChunk>(stages + kUpdChunk * kStride, B, ldb, 0, tid);
+  cp_async_commit();
+#pragma unroll 4
+  for (int i = 0; i < (kBlock * 64) / kGemmThreads; ++i) {
+    const int piece = tid + i * kGemmThreads;
+    cp_async16(Cs + (piece >> 6) * kStride + (piece & 63) * 2, Cg + (long long)(piece >> 6) * ldc + (piece & 63) * 2);
+  }
+  cp_async_commit();
+  for (int c = 0; c < nchunks; ++c) {
+    if (c + 1 < nchunks) {
+      double* next = stages + ((c + 1) & 1) * kStage;
+      stage_rows<kUpdChunk>(next, A, lda, (c + 1) * kUpdChunk, tid);
+      stage_rows<kUpdChunk>(next + kUpdChunk * kStride, B, ldb, (c + 1) * kUpdChunk, tid);
+      cp_async_commit();
+    }
+    // groups newer than chunk c that may stay in flight: c = 0 -> C tile and chunk 1;
+    // later -> chunk c + 1 only; the last chunk waits for everything
+    if (c + 1 >= nchunks) {
+      cp_async_wait<0>();
+    } else if (c == 0) {
+      cp_async_wait<2>();
+    } else {
+      cp_async_wait<1>();
+    }
+    __syncthreads();
+    const double* cur = stages + (c & 1) * kStage;
+    mma_chunk_any(acc, cur, cur + kUpdChunk * kStride, warp, lane);
+    __syncthreads();
+  }
+}
+
+// Epilogue of an update tile: Cs[row][col] -= acc in the accumulator's own fragment layout
+// and, for an off-diagonal tile of the symmetric sweep (`mirror`), the new value also goes
+// straight from registers to its transposed position M[c0 + col][r0 + row] of Mt (= M at
+// row c0, column r0): the 8 lanes sharing a column write 8 consecutive rows, i.e. whole 64-byte
+// segments, so the transpose needs no conflicting column reads of shared memory.
+__device__ __forceinline__ void acc_sub_smem(const TileAcc& acc, double* Cs, double* Mt, long long ld, bool mirror) {
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  const int wm = (warp >> 2) * 64;
+  const int wn = (warp & 3) * 32;
+#pragma unroll
+  for (int mt = 0; mt < 8; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      const int row = wm + mt * 8 + (lane >> 2), col = wn + nt * 8 + 2 * (lane & 3);
+      double* d = Cs + row * kStride + col;
+      const double v0 = d[0] - acc.v[mt][nt][0], v1 = d[1] - acc.v[mt][nt][1];
+      d[0] = v0;
+      d[1] = v1;
+      if (mirror) {
+        Mt[(long long)col * ld + row] = v0;
+        Mt[(long long)(col + 1) * ld + row] = v1;
+      }
+    }
+}
+__device__ __forceinline__ void acc_sub_smem(const TileAcc32& acc, double* Cs, double* Mt, long long ld, bool mirror) {
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  const int wm = (warp >> 2) * 64;
+  const int wn = (warp & 3) * 32;
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int row = wm + mt * 16 + g + 8 * h, col = wn + nt * 8 + 2 * t;
+        double* d = Cs + row * kStride + col;
+        const double v0 = d[0] - acc.v[mt][nt][2 * h], v1 = d[1] - acc.v[mt][nt][2 * h + 1];
+        d[0] = v0;
+        d[1] = v1;
+        if (mirror) {
+          Mt[(long long)col * ld + row] = v0;
+          Mt[(long long)(col + 1) * ld + row] = v1;
+        }
+      }
 }
 
 }  // namespace ticc

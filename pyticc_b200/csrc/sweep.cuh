@@ -27,7 +27,8 @@ constexpr int kPivotLd = kStride;  // the pivot block lives in a [128][kStride] 
 constexpr int kSub = 64;           // Gauss-Jordan sub-block of the pivot block
 constexpr size_t kPivotAuxBytes = size_t(2) * kSub * kSub * sizeof(double) + 2 * kSub * sizeof(double) + 4 * sizeof(double) + (4 + kSub) * sizeof(int);
 constexpr size_t kPivotSmemBytes = size_t(kBlock) * kPivotLd * sizeof(double) + kPivotAuxBytes;
-constexpr size_t kUpdateSmemBytes = kTileSmemBytes + kPivotAuxBytes;
+constexpr size_t kUpdateSmemBytes = kUpdTileSmemBytes;  // stages + C tile; the pivot aux reuses the stages
+static_assert(kPivotAuxBytes <= size_t(kUpdStageDoubles) * sizeof(double), "pivot scratch must fit in the update stages");
 
 // Gauss-Jordan exchange of a 64x64 sub-block S (row stride kPivotLd) with partial
 // pivoting over its rows, by the kPivotThreads threads of the CTA; writes the inverse in
@@ -394,37 +395,38 @@ __global__ void __launch_bounds__(kGemmThreads) sweep_update_kernel(double* __re
   double* Mb = M + (long long)b * mstride;
   const double* Cb = cold + (long long)b * cstride;
   const int tid = threadIdx.x;
-  // pull this tile of M towards L2 while the product runs
-  for (int line = tid; line < kBlock * 8; line += kGemmThreads) {
-    const double* addr = Mb + (long long)(r0 + (line >> 3)) * ld + c0 + (line & 7) * 16;
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(addr));
-  }
+  // shared memory: [A/B stages | C tile]; the C tile is staged during the product and the
+  // pivot inversion below reuses the stage region as its scratch
+  double* Cs = smem + kUpdStageDoubles;
+  const double* Cg = Mb + (long long)r0 * ld + c0;
   // the leading `*reduced_blocks` pivot blocks (channels closed beyond the threshold of the
   // mixed-precision mode) take the FP32-accurate TF32x3 product; all others FP64 DMMA
+  // off-diagonal tiles of the symmetric sweep write their transpose from registers
+  const bool mirror = kSym && r0 != c0;
+  double* Mt = Mb + (long long)c0 * ld + r0;
   if (reduced_blocks != nullptr && kb < *reduced_blocks) {
     TileAcc32 acc;
-    tile_gemm_tn_tf32x3(acc, Cb + r0, ld, Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
-    acc32_to_smem(acc, smem, -1.0);
+    tile_update_product(acc, Cb + r0, ld, Mb + (long long)k0 * ld + c0, ld, kBlock, smem, Cs, Cg, ld);
+    acc_sub_smem(acc, Cs, Mt, ld, mirror);
   } else {
     TileAcc acc;
-    tile_gemm_tn(acc, Cb + r0, ld, Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
-    acc_to_smem(acc, smem, -1.0);
+    tile_update_product(acc, Cb + r0, ld, Mb + (long long)k0 * ld + c0, ld, kBlock, smem, Cs, Cg, ld);
+    acc_sub_smem(acc, Cs, Mt, ld, mirror);
   }
   __syncthreads();
-  add_tile_from_global(smem, Mb, ld, r0, c0);
-  __syncthreads();
   if (!next_pivot) {
-    store_tile(Mb, ld, r0, c0, smem, kSym);
+    // rows from shared memory; a diagonal tile is written symmetrised from its lower half
+    store_tile(Mb, ld, r0, c0, Cs, kSym && r0 == c0);
     return;
   }
   if (kSym) {  // symmetrise the pivot block from its lower half, as store_tile would
     for (int e = tid; e < kBlock * kBlock; e += kGemmThreads) {
       const int r = e >> 7, c = e & (kBlock - 1);
-      if (r < c) smem[r * kStride + c] = smem[c * kStride + r];
+      if (r < c) Cs[r * kStride + c] = Cs[c * kStride + r];
     }
     __syncthreads();
   }
-  invert_pivot_block<kSym>(smem, smem + kBlock * kStride, Mb, ld, r0, pinv, b, status);
+  invert_pivot_block<kSym>(Cs, smem, Mb, ld, r0, pinv, b, status);
 }
 
 // Scratch per matrix: cold (kBlock x np) + P^-1 and its transpose (2 x kBlock x kBlock).
