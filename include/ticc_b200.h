@@ -68,7 +68,7 @@ int ticc_sym_inverse(void* M, int n, int batch, int is_complex, void* workspace,
  * there), plugin hosts that pass only buffers they own, and C/Fortran drivers without a
  * device allocator.  It has no counterpart in the reference.  Scratch comes from a fixed
  * 32 MiB device array inside the library (held by every GPU that loads it until the
- * process exits), so batch * (Np^2 + 128 Np + 32768) doubles must fit in 32 MiB, with
+ * process exits), so batch * (Np^2 + 128 Np + 32784) doubles must fit in 32 MiB, with
  * Np = n (2n when complex) rounded up to 128 — e.g. n <= 512 with batch <= 11; larger
  * requests are rejected with TICC_ERR_INVALID_ARGUMENT and a message.  The first call on
  * a device looks up the array's device address (cudaGetSymbolAddress) with that device

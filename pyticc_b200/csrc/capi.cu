@@ -454,7 +454,7 @@ int ticc_sym_inverse_noalloc(void* M, int n, int batch, int is_complex, int* dev
   if (need > kNoAllocScratchBytes)
     return fail(TICC_ERR_INVALID_ARGUMENT,
                 "ticc_sym_inverse_noalloc: n=%d batch=%d is_complex=%d needs %zu bytes of scratch, but the fixed device array holds %zu bytes "
-                "(batch * (Np^2 + 128 Np + 32768) doubles with Np = n, or 2n when complex, rounded up to 128)",
+                "(batch * (Np^2 + 128 Np + 32784) doubles with Np = n, or 2n when complex, rounded up to 128)",
                 n, batch, is_complex, need, kNoAllocScratchBytes);
   int device = 0;
   cudaError_t e = cudaGetDevice(&device);

@@ -259,27 +259,37 @@ __device__ __forceinline__ void acc_zero(TileAcc32& acc) {
       for (int q = 0; q < 4; ++q) acc.v[mt][nt][q] = 0.0f;
 }
 
-// acc = sum_{k < K} A[k][.]^T B[k][.] (K a multiple of kUpdChunk, at least 2 chunks) while
-// Cs <- C[r][c] for the 128 x 128 tile at Cg (row stride ldc).  On return Cs holds C and the
-// staging region is free (ends with a __syncthreads()).
-template <class Acc>
-__device__ inline void tile_update_product(Acc& acc, const double* A, long long lda, const double* B, long long ldb, int K, double* stages, double* Cs, const double* Cg, long long ldc) {
+// The product is split so that a persistent CTA can start the next tile's loads early:
+// issue_update_chunk0 and issue_update_ctile each commit one cp.async group, and
+// update_mainloop expects exactly that order of groups in flight (chunk 0, C tile) and
+// then commits chunks 1 .. K/kUpdChunk - 1 itself.
+__device__ __forceinline__ void issue_update_chunk0(const double* A, long long lda, const double* B, long long ldb, double* stages) {
   const int tid = threadIdx.x;
-  const int warp = tid >> 5;
-  const int lane = tid & 31;
-  acc_zero(acc);
-  constexpr int kStage = 2 * kUpdChunk * kStride;
-  const int nchunks = K / kUpdChunk;
-  // commit groups in order: chunk 0, C tile, chunk 1, chunk 2, ...
   stage_rows<kUpdChunk>(stages, A, lda, 0, tid);
   stage_rows<kUpdChunk>(stages + kUpdChunk * kStride, B, ldb, 0, tid);
   cp_async_commit();
+}
+__device__ __forceinline__ void issue_update_ctile(double* Cs, const double* Cg, long long ldc) {
+  const int tid = threadIdx.x;
 #pragma unroll 4
   for (int i = 0; i < (kBlock * 64) / kGemmThreads; ++i) {
     const int piece = tid + i * kGemmThreads;
     cp_async16(Cs + (piece >> 6) * kStride + (piece & 63) * 2, Cg + (long long)(piece >> 6) * ldc + (piece & 63) * 2);
   }
   cp_async_commit();
+}
+
+// acc = sum_{k < K} A[k][.]^T B[k][.] (K a multiple of kUpdChunk, at least 2 chunks), with
+// chunk 0 and the C tile already issued.  On return Cs holds C and the staging region is
+// free (ends with a __syncthreads()).
+template <class Acc>
+__device__ inline void update_mainloop(Acc& acc, const double* A, long long lda, const double* B, long long ldb, int K, double* stages) {
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  acc_zero(acc);
+  constexpr int kStage = 2 * kUpdChunk * kStride;
+  const int nchunks = K / kUpdChunk;
   for (int c = 0; c < nchunks; ++c) {
     if (c + 1 < nchunks) {
       double* next = stages + ((c + 1) & 1) * kStage;
@@ -301,6 +311,14 @@ __device__ inline void tile_update_product(Acc& acc, const double* A, long long 
     mma_chunk_any(acc, cur, cur + kUpdChunk * kStride, warp, lane);
     __syncthreads();
   }
+}
+
+// The whole product in one call: Cs <- C tile while acc = A^T B.
+template <class Acc>
+__device__ inline void tile_update_product(Acc& acc, const double* A, long long lda, const double* B, long long ldb, int K, double* stages, double* Cs, const double* Cg, long long ldc) {
+  issue_update_chunk0(A, lda, B, ldb, stages);
+  issue_update_ctile(Cs, Cg, ldc);
+  update_mainloop(acc, A, lda, B, ldb, K, stages);
 }
 
 // Epilogue of an update tile: Cs[row][col] -= acc in the accumulator's own fragment layout

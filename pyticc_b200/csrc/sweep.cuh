@@ -27,7 +27,7 @@ constexpr int kPivotLd = kStride;  // the pivot block lives in a [128][kStride] 
 constexpr int kSub = 64;           // Gauss-Jordan sub-block of the pivot block
 constexpr size_t kPivotAuxBytes = size_t(2) * kSub * kSub * sizeof(double) + 2 * kSub * sizeof(double) + 4 * sizeof(double) + (4 + kSub) * sizeof(int);
 constexpr size_t kPivotSmemBytes = size_t(kBlock) * kPivotLd * sizeof(double) + kPivotAuxBytes;
-constexpr size_t kUpdateSmemBytes = kUpdTileSmemBytes;  // stages + C tile; the pivot aux reuses the stages
+constexpr size_t kUpdateSmemBytes = kUpdTileSmemBytes + 16;  // + the broadcast slot of the tile queue  // stages + C tile; the pivot aux reuses the stages
 static_assert(kPivotAuxBytes <= size_t(kUpdStageDoubles) * sizeof(double), "pivot scratch must fit in the update stages");
 
 // Gauss-Jordan exchange of a 64x64 sub-block S (row stride kPivotLd) with partial
@@ -306,7 +306,7 @@ __device__ inline void store_tile(double* Mb, int ld, int r0, int c0, const doub
 // sweep also keeps the old rows (= old columns K, transposed) in `cold` and mirrors U^T
 // into the columns K; the general sweep leaves the columns to the column-panel kernel.
 template <bool kSym>
-__global__ void __launch_bounds__(kGemmThreads) sweep_rowpanel_kernel(double* __restrict__ M, long long mstride, int ld, int kb, const double* __restrict__ pinv, double* __restrict__ cold, long long cstride) {
+__global__ void __launch_bounds__(kGemmThreads) sweep_rowpanel_kernel(double* __restrict__ M, long long mstride, int ld, int kb, const double* __restrict__ pinv, double* __restrict__ cold, long long cstride, int* queue) {
   extern __shared__ double smem[];
   const int b = blockIdx.y;
   const int jt = blockIdx.x + (blockIdx.x >= kb ? 1 : 0);
@@ -321,6 +321,7 @@ __global__ void __launch_bounds__(kGemmThreads) sweep_rowpanel_kernel(double* __
   acc_to_smem(acc, smem, 1.0);
   __syncthreads();
   store_tile(Mb, ld, k0, c0, smem, kSym);
+  if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) *queue = 0;  // the step's update tile queue
 }
 
 // Column panel of the general sweep: M_RK <- M_RK P^-1 for one 128-row tile, keeping
@@ -360,77 +361,133 @@ __device__ __forceinline__ void lower_pair(int idx, int& a, int& b) {
   b = idx - r * (r + 1) / 2;
 }
 
-// Trailing update M_RR -= cold^T U: the symmetric sweep visits the lower-triangular
-// tiles and mirrors them, the general sweep visits every tile.  The grid is linear:
-// its first `batch` CTAs own the next pivot block (kb+1, kb+1) of each matrix and,
-// after their tile, invert it in place while the other CTAs finish the update, so the
-// next step's row panel starts without a separate pivot launch.
+// Matrix b and lower (symmetric sweep) or any (general sweep) tile (ta, tb) of update item g,
+// skipping the pivot row/column kb.
 template <bool kSym>
-__global__ void __launch_bounds__(kGemmThreads) sweep_update_kernel(double* __restrict__ M, long long mstride, int ld, int kb, const double* __restrict__ cold, long long cstride, int tiles_per_dim, int batch, int fuse_next, double* __restrict__ pinv, int* status, const int* __restrict__ reduced_blocks) {
+__device__ __forceinline__ void update_tile_of(int g, int per, int t, int kb, int& b, int& ta, int& tb) {
+  b = g / per;
+  const int local = g - b * per;
+  if (kSym) {
+    lower_pair(local, ta, tb);
+  } else {
+    ta = local / t;
+    tb = local % t;
+  }
+  ta += (ta >= kb) ? 1 : 0;
+  tb += (tb >= kb) ? 1 : 0;
+}
+
+// Persistent tile loop of the trailing update: tiles come from the step's atomic queue; the
+// next tile's first K-chunk is issued before the current tile's epilogue and its C tile
+// right after, so only the product itself is on the critical path of a CTA.
+template <bool kSym, class Acc>
+__device__ inline void update_tiles(double* M, long long mstride, int ld, int kb, const double* cold, long long cstride, int t, int per, int total, bool skip_pivot, int* queue,
+                                    double* smem) {
+  const int tid = threadIdx.x;
+  double* Cs = smem + kUpdStageDoubles;
+  int* slot = reinterpret_cast<int*>(Cs + kBlock * kStride);
+  const int k0 = kb * kBlock;
+  auto fetch = [&]() {
+    if (tid == 0) {
+      int g = atomicAdd(queue, 1);
+      for (;;) {
+        if (g >= total || !skip_pivot) break;
+        int b, ta, tb;
+        update_tile_of<kSym>(g, per, t, kb, b, ta, tb);
+        if (ta != kb + 1 || tb != kb + 1) break;
+        g = atomicAdd(queue, 1);  // the pivot tile belongs to a pivot CTA
+      }
+      *slot = g;
+    }
+    __syncthreads();
+    const int g = *slot;
+    __syncthreads();
+    return g;
+  };
+  int g = fetch();
+  if (g >= total) return;
+  int b, ta, tb;
+  update_tile_of<kSym>(g, per, t, kb, b, ta, tb);
+  issue_update_chunk0(cold + (long long)b * cstride + ta * kBlock, ld, M + (long long)b * mstride + (long long)k0 * ld + tb * kBlock, ld, smem);
+  issue_update_ctile(Cs, M + (long long)b * mstride + (long long)ta * kBlock * ld + tb * kBlock, ld);
+  for (;;) {
+    double* Mb = M + (long long)b * mstride;
+    const int r0 = ta * kBlock, c0 = tb * kBlock;
+    Acc acc;
+    update_mainloop(acc, cold + (long long)b * cstride + r0, ld, Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
+    const int gn = fetch();
+    int bn = 0, tan = 0, tbn = 0;
+    if (gn < total) {
+      update_tile_of<kSym>(gn, per, t, kb, bn, tan, tbn);
+      issue_update_chunk0(cold + (long long)bn * cstride + tan * kBlock, ld, M + (long long)bn * mstride + (long long)k0 * ld + tbn * kBlock, ld, smem);
+    }
+    // off-diagonal tiles of the symmetric sweep write their transpose from registers
+    acc_sub_smem(acc, Cs, Mb + (long long)c0 * ld + r0, ld, kSym && r0 != c0);
+    __syncthreads();
+    store_tile(Mb, ld, r0, c0, Cs, kSym && r0 == c0);  // a diagonal tile symmetrised from its lower half
+    __syncthreads();
+    if (gn >= total) break;
+    issue_update_ctile(Cs, M + (long long)bn * mstride + (long long)tan * kBlock * ld + tbn * kBlock, ld);
+    b = bn;
+    ta = tan;
+    tb = tbn;
+  }
+}
+
+// Trailing update M_RR -= cold^T U: the symmetric sweep visits the lower-triangular tiles
+// and mirrors them, the general sweep visits every tile.  Persistent: about one CTA per SM.
+// The first `batch` CTAs first update the next pivot block (kb+1, kb+1) of their matrix and
+// invert it in place, so the next step's row panel needs no separate pivot launch, then
+// join the tile queue (reset to 0 by this step's row-panel kernel).
+template <bool kSym>
+__global__ void __launch_bounds__(kGemmThreads, 1) sweep_update_kernel(double* __restrict__ M, long long mstride, int ld, int kb, const double* __restrict__ cold, long long cstride, int tiles_per_dim, int batch, int fuse_next, double* __restrict__ pinv, int* status, const int* __restrict__ reduced_blocks, int* queue) {
   extern __shared__ double smem[];
   const int t = tiles_per_dim;  // tiles per dimension excluding the pivot block kb
   const int per = kSym ? t * (t + 1) / 2 : t * t;
-  int b, ta, tb;
-  bool next_pivot = false;
-  long long idx = blockIdx.x;
-  if (fuse_next && idx < batch) {
-    b = (int)idx;
-    ta = tb = kb + 1;
-    next_pivot = true;
-  } else {
-    if (fuse_next) idx -= batch;
-    b = (int)(idx / per);
-    int local = (int)(idx % per);
-    if (kSym) {
-      lower_pair(local, ta, tb);
-    } else {
-      ta = local / t;
-      tb = local % t;
-    }
-    ta += (ta >= kb) ? 1 : 0;
-    tb += (tb >= kb) ? 1 : 0;
-    if (fuse_next && ta == kb + 1 && tb == kb + 1) return;  // owned by a pivot CTA
-  }
-  const int r0 = ta * kBlock, c0 = tb * kBlock, k0 = kb * kBlock;
-  double* Mb = M + (long long)b * mstride;
-  const double* Cb = cold + (long long)b * cstride;
+  const int total = per * batch;
   const int tid = threadIdx.x;
-  // shared memory: [A/B stages | C tile]; the C tile is staged during the product and the
-  // pivot inversion below reuses the stage region as its scratch
-  double* Cs = smem + kUpdStageDoubles;
-  const double* Cg = Mb + (long long)r0 * ld + c0;
+  const int k0 = kb * kBlock;
+  double* Cs = smem + kUpdStageDoubles;  // [A/B stages | C tile]; the inversion's scratch reuses the stages
   // the leading `*reduced_blocks` pivot blocks (channels closed beyond the threshold of the
   // mixed-precision mode) take the FP32-accurate TF32x3 product; all others FP64 DMMA
-  // off-diagonal tiles of the symmetric sweep write their transpose from registers
-  const bool mirror = kSym && r0 != c0;
-  double* Mt = Mb + (long long)c0 * ld + r0;
-  if (reduced_blocks != nullptr && kb < *reduced_blocks) {
-    TileAcc32 acc;
-    tile_update_product(acc, Cb + r0, ld, Mb + (long long)k0 * ld + c0, ld, kBlock, smem, Cs, Cg, ld);
-    acc_sub_smem(acc, Cs, Mt, ld, mirror);
-  } else {
-    TileAcc acc;
-    tile_update_product(acc, Cb + r0, ld, Mb + (long long)k0 * ld + c0, ld, kBlock, smem, Cs, Cg, ld);
-    acc_sub_smem(acc, Cs, Mt, ld, mirror);
-  }
-  __syncthreads();
-  if (!next_pivot) {
-    // rows from shared memory; a diagonal tile is written symmetrised from its lower half
-    store_tile(Mb, ld, r0, c0, Cs, kSym && r0 == c0);
-    return;
-  }
-  if (kSym) {  // symmetrise the pivot block from its lower half, as store_tile would
-    for (int e = tid; e < kBlock * kBlock; e += kGemmThreads) {
-      const int r = e >> 7, c = e & (kBlock - 1);
-      if (r < c) Cs[r * kStride + c] = Cs[c * kStride + r];
+  const bool reduced = reduced_blocks != nullptr && kb < *reduced_blocks;
+  if (fuse_next && (int)blockIdx.x < batch) {
+    const int b = blockIdx.x;
+    const int p0 = (kb + 1) * kBlock;
+    double* Mb = M + (long long)b * mstride;
+    const double* A = cold + (long long)b * cstride + p0;
+    const double* B = Mb + (long long)k0 * ld + p0;
+    const double* Cg = Mb + (long long)p0 * ld + p0;
+    if (reduced) {
+      TileAcc32 acc;
+      tile_update_product(acc, A, ld, B, ld, kBlock, smem, Cs, Cg, ld);
+      acc_sub_smem(acc, Cs, Mb, ld, false);
+    } else {
+      TileAcc acc;
+      tile_update_product(acc, A, ld, B, ld, kBlock, smem, Cs, Cg, ld);
+      acc_sub_smem(acc, Cs, Mb, ld, false);
     }
     __syncthreads();
+    if (kSym) {  // symmetrise the pivot block from its lower half, as store_tile would
+      for (int e = tid; e < kBlock * kBlock; e += kGemmThreads) {
+        const int r = e >> 7, c = e & (kBlock - 1);
+        if (r < c) Cs[r * kStride + c] = Cs[c * kStride + r];
+      }
+      __syncthreads();
+    }
+    invert_pivot_block<kSym>(Cs, smem, Mb, ld, p0, pinv, b, status);
+    __syncthreads();
   }
-  invert_pivot_block<kSym>(Cs, smem, Mb, ld, r0, pinv, b, status);
+  if (reduced) {
+    update_tiles<kSym, TileAcc32>(M, mstride, ld, kb, cold, cstride, t, per, total, fuse_next != 0, queue, smem);
+  } else {
+    update_tiles<kSym, TileAcc>(M, mstride, ld, kb, cold, cstride, t, per, total, fuse_next != 0, queue, smem);
+  }
 }
 
 // Scratch per matrix: cold (kBlock x np) + P^-1 and its transpose (2 x kBlock x kBlock).
-inline size_t sweep_scratch_doubles(int np) { return size_t(kBlock) * np + size_t(2) * kBlock * kBlock; }
+// The last 16 doubles of each matrix's share hold the update kernel's tile queue (one int).
+inline size_t sweep_scratch_doubles(int np) { return size_t(kBlock) * np + size_t(2) * kBlock * kBlock + 16; }
 
 template <bool kSym>
 inline cudaError_t sweep_configure_variant() {
@@ -462,19 +519,32 @@ inline cudaError_t sweep_batched(double* M, long long mstride, int np, int batch
   const long long cstride = (long long)kBlock * np;
   double* cold = scratch;
   double* pinv = scratch + (long long)batch * cstride;
+  int* queue = reinterpret_cast<int*>(pinv + (long long)batch * 2 * kBlock * kBlock);
+  int sms = 0;
+  if (nt > 1) {
+    int dev = 0;
+    e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+  }
   sweep_pivot_kernel<kSym><<<batch, kPivotThreads, kPivotSmemBytes, stream>>>(M, mstride, np, 0, pinv, status);
   note_launch();
   for (int kb = 0; kb < nt; ++kb) {
     if (nt == 1) break;
     const int t = nt - 1;
-    sweep_rowpanel_kernel<kSym><<<dim3(t, batch), kGemmThreads, kTileSmemBytes, stream>>>(M, mstride, np, kb, pinv, cold, cstride);
+    sweep_rowpanel_kernel<kSym><<<dim3(t, batch), kGemmThreads, kTileSmemBytes, stream>>>(M, mstride, np, kb, pinv, cold, cstride, queue);
     note_launch();
-    if (!kSym) sweep_colpanel_kernel<<<dim3(t, batch), kGemmThreads, kTileSmemBytes, stream>>>(M, mstride, np, kb, pinv, cold, cstride);
-    note_launch();
+    if (!kSym) {
+      sweep_colpanel_kernel<<<dim3(t, batch), kGemmThreads, kTileSmemBytes, stream>>>(M, mstride, np, kb, pinv, cold, cstride);
+      note_launch();
+    }
     const int per = kSym ? t * (t + 1) / 2 : t * t;
     const int fuse = (kb + 1 < nt) ? 1 : 0;
-    const long long blocks = (long long)per * batch + (fuse ? batch : 0);
-    sweep_update_kernel<kSym><<<(unsigned)blocks, kGemmThreads, kUpdateSmemBytes, stream>>>(M, mstride, np, kb, cold, cstride, t, batch, fuse, pinv, status, reduced_blocks);
+    // persistent grid: one CTA per SM (shared memory allows no second), at least one per pivot
+    const long long work = (long long)per * batch + (fuse ? batch : 0);
+    long long blocks = work < sms ? work : sms;
+    if (fuse && blocks < batch) blocks = batch;
+    sweep_update_kernel<kSym><<<(unsigned)blocks, kGemmThreads, kUpdateSmemBytes, stream>>>(M, mstride, np, kb, cold, cstride, t, batch, fuse, pinv, status, reduced_blocks, queue);
     note_launch();
   }
   return cudaGetLastError();
