@@ -39,7 +39,9 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["native", "reference"], default="native")
     p.add_argument("--batch", type=int, default=16, help="energies per step")
-    p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    p.add_argument("--precision", choices=["fp64", "mixed"], default="mixed", help="headline arm precision")
+    p.add_argument("--schedule", choices=["fixed", "learned"], default="learned", help="headline arm sector schedule")
+    p.add_argument("--plain-steps", type=int, default=None, help="timed steps of the plain FP64 fixed-step arm (default: steps - 1, at least 1)")
     p.add_argument("--sectors", type=int, default=0, help="limit sectors (0 = all 938); for quick checks only")
     return p.parse_args()
 
@@ -212,6 +214,8 @@ def main():
     from pyticc_b200 import _native as nat
     from pyticc_b200 import scattering
     from pyticc_b200.propagation import runner
+    from pyticc_b200.propagation.learned import learned_sectors, resolve_proposer
+    from pyticc_b200.replicas import max_over_ranks
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -226,44 +230,65 @@ def main():
     lib = nat.load_library()
     blocks = build_workload(args)
     sectors_of = [b.grid.sectors if args.sectors == 0 else b.grid.sectors[: args.sectors] for b in blocks]
-    config = tb.Propagation(precision=args.precision)
+    proposer = resolve_proposer(None)
+    headline = tb.Propagation(precision=args.precision)
+    plain = tb.Propagation(precision="fp64")
+    plain_steps = args.plain_steps if args.plain_steps is not None else max(1, args.steps - 1)
     n_total = args.warmup + args.steps
     plan = units(blocks, args.batch, rank, world, n_total)
 
-    def one_step(block_index, energy_slice, timing_list=None):
+    def one_step(block_index, energy_slice, config, schedule, timing_list=None, used=None):
+        """One solve batch through the library's device path: schedule, propagate, match."""
         wl = blocks[block_index]
         ham = scattering.hamiltonian_for(wl.system, wl.grid)
         energies = wl.energies[energy_slice]
-        Y = runner.propagate(ham, energies, sectors_of[block_index], config, window_timing=timing_list)
+        sectors = sectors_of[block_index]
+        if schedule == "learned":
+            sectors = learned_sectors(ham, sectors, energies, proposer, "auto")
+        if used is not None:
+            used.append(len(sectors))
+        Y = runner.propagate(ham, energies, sectors, config, window_timing=timing_list)
         B, L = tb.get_Bmat_BF_to_SF(wl.system.basis)
         Y_sf = tb.match.asymptotic.transform_device(Y, nat.as_device(B, dev, torch.float64))
-        S, n_open = tb.match.smatrix.get_Smat_device(Y_sf, sectors_of[block_index][-1].radial_end, energies, ham.reduced_mass, wl.system.basis.E_int, L)
-        return S
+        S, n_open = tb.match.smatrix.get_Smat_device(Y_sf, sectors[-1].radial_end, energies, ham.reduced_mass, wl.system.basis.E_int, L)
+        return S, n_open
 
-    # warm-up (also builds and caches the Hamiltonian rows and device PES grids)
-    for k in range(args.warmup):
-        one_step(*plan[k])
-    torch.cuda.synchronize()
-    launches0 = lib.ticc_kernel_launches()
-    windows: list = []
-    if group:
-        group.barrier()
-    torch.cuda.synchronize()
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
+    def timed(config, schedule, steps, warmup, windows=None, used=None):
+        for k in range(warmup):
+            one_step(*plan[k], config, schedule)
+        torch.cuda.synchronize()
+        if group:
+            group.barrier()
+        torch.cuda.synchronize()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        first = None
         start.record()
-        for k in range(args.warmup, n_total):
-            one_step(*plan[k], timing_list=windows)
+        for k in range(warmup, warmup + steps):
+            out = one_step(*plan[k], config, schedule, timing_list=windows, used=used)
+            first = out if first is None else first
         stop.record()
         torch.cuda.synchronize()
-    if group:
-        group.barrier()
-    launches = lib.ticc_kernel_launches() - launches0
-    from pyticc_b200.replicas import max_over_ranks
+        if group:
+            group.barrier()
+        return max_over_ranks(start.elapsed_time(stop) * 1e-3, group), first
 
-    elapsed = max_over_ranks(start.elapsed_time(stop) * 1e-3, group)
+    # headline arm: mixed precision + learned sector widths (warm-up also builds the
+    # Hamiltonian rows and device PES grids)
+    launches0 = None
+    windows: list = []
+    used: list = []
+    for k in range(args.warmup):
+        one_step(*plan[k], headline, args.schedule)
+    torch.cuda.synchronize()
+    launches0 = lib.ticc_kernel_launches()
+    with ClockSampler(local) as clocks:
+        elapsed, head_first = timed(headline, args.schedule, args.steps, 0, windows, used)
+    launches = lib.ticc_kernel_launches() - launches0
     solves = args.steps * args.batch * world
     value = solves / elapsed
+    # plain FP64 fixed-step arm on the same first units (its kernels are warm)
+    plain_elapsed, plain_first = timed(plain, "fixed", plain_steps, 0)
+    plain_value = plain_steps * args.batch * world / plain_elapsed
 
     # roofline: the LDMD propagate launches (window x energy batch), two symmetric
     # N x N inversions (N^3 flops each) per (sector, energy)
@@ -271,10 +296,16 @@ def main():
     prop_flops = sum(f for _, _, f in windows)
     peak = fp64_peak_tflops(torch, dev) if rank == 0 else 0.0
 
+    # accuracy of the headline arm against plain FP64 fixed step on the first timed unit
+    S_h, n_h = head_first
+    S_p, n_p = plain_first
+    counts_equal = bool(np.array_equal(np.asarray(n_h), np.asarray(n_p)))
+    max_dS = float((S_h - S_p).abs().max().item())
+
     # end-to-end through the public API: host energies in, host S and Y out, fresh device PES copy
     e2e_value = None
-    max_dS = None
     h2d = d2h = 0
+    cpu = None
     if rank == 0:
         wl = blocks[plan[args.warmup][0]]
         energies = np.ascontiguousarray(wl.energies[plan[args.warmup][1]])
@@ -282,15 +313,13 @@ def main():
         runner._DEVICE_HAMILTONIANS.clear()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        result = tb.solve(wl.system, energies, wl.grid, config, sectors=sectors_of[plan[args.warmup][0]])
+        e2e_config = tb.Propagation(precision=args.precision, steps=args.schedule)
+        result = tb.solve(wl.system, energies, wl.grid, e2e_config, sectors=None if args.sectors == 0 else sectors_of[plan[args.warmup][0]])
         e2e_seconds = time.perf_counter() - t0
         e2e_value = len(energies) / e2e_seconds
         h2d = int(energies.nbytes + wl.grid.values.nbytes)
-        d2h = int(result.Y_propagated.nbytes + sum(s.nbytes for s in result.Smat))
+        d2h = int(result.Y_propagated.nbytes + sum(x.nbytes for x in result.Smat))
         cpu = cpu_baseline(wl, energies)
-        if args.precision == "mixed":
-            plain = tb.solve(wl.system, energies, wl.grid, tb.Propagation(), sectors=sectors_of[plan[args.warmup][0]])
-            max_dS = max(float(np.abs(a - b).max()) for a, b in zip(plain.Smat, result.Smat, strict=True) if a.size)
     if group:
         group.barrier()
         group.destroy_process_group()
@@ -298,6 +327,7 @@ def main():
         return
     n_channel = blocks[0].system.basis.n_channel
     achieved = prop_flops / prop_seconds / 1e12 if prop_seconds else None
+    n_fixed = len(sectors_of[0])
     line = {
         "metric": METRIC,
         "value": value,
@@ -309,15 +339,20 @@ def main():
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f64" if args.precision == "fp64" else "f64+tf32x3",
         "data": "synthetic",
         "config": {
             "workload": WORKLOAD,
             "batch": args.batch,
             "precision": args.precision,
-            "schedule": "fixed h=0.02" if args.sectors == 0 else f"first {args.sectors} sectors",
+            "schedule": args.schedule,
+            "sectors_fixed": n_fixed,
+            "sectors_used_per_step": used,
             "l2": "inputs larger than L2 (per-energy work matrices 32 MiB each, W windows > 1 GiB)",
         },
+        "plain_fp64": {"value": plain_value, "unit": "solves/s", "steps": plain_steps, "ms_per_step": plain_elapsed / plain_steps * 1e3, "schedule": "fixed h=0.02",
+                       "speedup_of_value": value / plain_value},
+        "accuracy": {"max_dS_vs_plain_fp64": max_dS, "open_counts_equal": counts_equal, "tolerance": 1e-6, "energies": args.batch},
         "roofline": {
             "bound": "tensor",
             "achieved": achieved,
@@ -325,12 +360,11 @@ def main():
             "unit": "TFLOP/s",
             "frac": achieved / peak if achieved and peak else None,
             "traffic": None,
-            "kernel": "ticc_ldmd_propagate (batched symmetric sweeps on FP64 DMMA); peak = cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)",
-            "flops_per_unit": f"2 N^3 per (sector, energy), N={n_channel}",
+            "kernel": "ticc_ldmd_propagate of the headline arm (batched symmetric sweeps; FP64 DMMA, TF32x3 on strongly closed blocks in mixed precision); peak = cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)",
+            "flops_per_unit": f"2 N^3 per (sector, energy), N={n_channel}, counted in FP64-equivalent flops",
         },
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "accuracy": {"max_dS_vs_plain_fp64": max_dS, "tolerance": 1e-6} if args.precision == "mixed" else None,
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
     }
