@@ -88,8 +88,10 @@ int ticc_sym_inverse_noalloc(void* M, int n, int batch, int is_complex, int* dev
  *   energies   device, n_energy total energies (hartree).
  *   half_steps device, n_sector half-steps (bohr), all > 0.
  *   W_start/W_mid/W_end device, energy-independent W_base at the sector start,
- *              midpoint and end, each n x n (symmetric) at the given element stride
- *              between consecutive sectors (e.g. 2*n*n for an interleaved point list).
+ *              midpoint and end, each n x n and exactly symmetric (only W[i][j] is read
+ *              for element (i, j); ticc_contract's W assembly produces such matrices), at
+ *              the given element stride between consecutive sectors (e.g. 2*n*n for an
+ *              interleaved point list).
  *   precision  TICC_PRECISION_FP64 (all-FP64) or TICC_PRECISION_MIXED: the trailing
  *              updates of the leading sweep blocks whose channels are all closed with a
  *              local wavenumber above 30 bohr^-1 at the batch's highest energy run as an

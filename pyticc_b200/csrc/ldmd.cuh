@@ -162,24 +162,56 @@ __device__ __forceinline__ void get_swept(const double* Mb, int np, int i, int j
 // Work-matrix padding: identity on the padded diagonal of the real sweep matrix.
 __device__ __forceinline__ void put_padding(double* Mb, int np, long long r, long long c) { Mb[r * np + c] = (r == c) ? 1.0 : 0.0; }
 
+// W_base must be exactly symmetric (the contraction writes both halves from one value), so
+// the per-energy passes read W[i][j] only, row-contiguous across the threads of a warp.
 // phase 0: A = Y_in + Q_start + y1          (first sector of the call)
 // phase 1: A = [Q_end' + y1' + y2' S y2'] + Q_start + y1   (S from the previous sector)
 // phase 2: B = 2 Q_mid + 2 y1 + y2 S y2
 // phase 3: Y_out = Q_end + y1 + y2 S y2     (last sector of the call)
-__global__ void ldmd_elementwise_kernel(int phase, int s, LdmdSectors sec, LdmdLayout L, const double* Yin, double* Yout) {
+// One CTA per (logical row i, energy): the row's reference values are read once, the
+// threads run along j (coalesced M, W and y2 accesses, no per-element index division).
+__global__ void __launch_bounds__(256) ldmd_elementwise_kernel(int phase, int s, LdmdSectors sec, LdmdLayout L, const double* Yin, double* Yout) {
+  const int i = blockIdx.x;
   const int e = blockIdx.y;
   const int n = L.n, np = L.np;
   const int nl = L.is_complex ? np / 2 : np;  // logical-element grid covering the padded matrix
   double* Mb = L.M + (long long)e * np * np;
+  if (i >= n) {  // padding row
+    if (phase == 3) return;
+    for (int j = threadIdx.x; j < nl; j += blockDim.x) {
+      if (L.is_complex) {
+        for (int a = 0; a < 2; ++a)
+          for (int b = 0; b < 2; ++b) put_padding(Mb, np, 2LL * i + a, 2LL * j + b);
+      } else {
+        put_padding(Mb, np, i, j);
+      }
+    }
+    return;
+  }
   const double h = sec.h[s];
   const double* y1 = L.y1 + ((long long)s * L.n_energy + e) * n;
   const double* y2 = L.y2 + ((long long)s * L.n_energy + e) * n;
-  const double* Ws = sec.Ws + s * sec.ws_stride;
+  const double* Ws = sec.Ws + s * sec.ws_stride + (long long)i * n;
   const double* Wm = sec.Wm + s * sec.wm_stride;
-  const double* We = sec.We + s * sec.we_stride;
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < (long long)nl * nl; idx += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(idx / nl), j = (int)(idx % nl);
-    if (i >= n || j >= n) {
+  const double* We = sec.We + s * sec.we_stride + (long long)i * n;
+  const double ref = Wm[(long long)i * n + i];
+  const double y1i = y1[i], y2i = y2[i];
+  // previous sector (phase 1)
+  double hp = 0.0, ref_p = 0.0, y1pi = 0.0, y2pi = 0.0;
+  const double* Wep = nullptr;
+  const double* y2p = nullptr;
+  if (phase == 1) {
+    hp = sec.h[s - 1];
+    Wep = sec.We + (s - 1) * sec.we_stride + (long long)i * n;
+    const double* y1p = L.y1 + ((long long)(s - 1) * L.n_energy + e) * n;
+    y2p = L.y2 + ((long long)(s - 1) * L.n_energy + e) * n;
+    ref_p = sec.Wm[(s - 1) * sec.wm_stride + (long long)i * n + i];
+    y1pi = y1p[i];
+    y2pi = y2p[i];
+  }
+  const double* Qrow = L.Qm + (long long)s * L.npr * L.npr + (long long)i * L.npr;
+  for (int j = threadIdx.x; j < nl; j += blockDim.x) {
+    if (j >= n) {  // padding column
       if (phase == 3) continue;
       if (L.is_complex) {
         for (int a = 0; a < 2; ++a)
@@ -201,34 +233,25 @@ __global__ void ldmd_elementwise_kernel(int phase, int s, LdmdSectors sec, LdmdL
         x = 0.5 * (Yb[(long long)i * n + j] + Yb[(long long)j * n + i]);
       }
     } else if (phase == 1) {
-      const double hp = sec.h[s - 1];
-      const double* Wep = sec.We + (s - 1) * sec.we_stride;
-      const double* Wmp = sec.Wm + (s - 1) * sec.wm_stride;
-      const double* y1p = L.y1 + ((long long)(s - 1) * L.n_energy + e) * n;
-      const double* y2p = L.y2 + ((long long)(s - 1) * L.n_energy + e) * n;
       double sr, si;
       get_swept(Mb, np, i, j, L.is_complex, sr, si);
-      const double ref_p = Wmp[(long long)i * n + i];
-      x = hp * (sym(Wep, n, i, j) - d * ref_p) / 3.0 + d * y1p[i] + y2p[i] * sr * y2p[j];
-      z = y2p[i] * si * y2p[j];
+      x = hp * (Wep[j] - d * ref_p) / 3.0 + d * y1pi + y2pi * sr * y2p[j];
+      z = y2pi * si * y2p[j];
     }
     if (phase <= 1) {
-      const double ref = Wm[(long long)i * n + i];
-      x += h * (sym(Ws, n, i, j) - d * ref) / 3.0 + d * y1[i];
+      x += h * (Ws[j] - d * ref) / 3.0 + d * y1i;
       put_element(Mb, np, i, j, x, z, L.is_complex);
     } else if (phase == 2) {
       double sr, si;
       get_swept(Mb, np, i, j, L.is_complex, sr, si);
-      const double q = L.Qm[(long long)s * L.npr * L.npr + (long long)i * L.npr + j];
-      x = 2.0 * q + 2.0 * d * y1[i] + y2[i] * sr * y2[j];
-      z = y2[i] * si * y2[j];
+      x = 2.0 * Qrow[j] + 2.0 * d * y1i + y2i * sr * y2[j];
+      z = y2i * si * y2[j];
       put_element(Mb, np, i, j, x, z, L.is_complex);
     } else {
       double sr, si;
       get_swept(Mb, np, i, j, L.is_complex, sr, si);
-      const double ref = Wm[(long long)i * n + i];
-      x = h * (sym(We, n, i, j) - d * ref) / 3.0 + d * y1[i] + y2[i] * sr * y2[j];
-      z = y2[i] * si * y2[j];
+      x = h * (We[j] - d * ref) / 3.0 + d * y1i + y2i * sr * y2[j];
+      z = y2i * si * y2[j];
       if (L.is_complex) {
         Yout[((long long)e * n * n + (long long)i * n + j) * 2] = x;
         Yout[((long long)e * n * n + (long long)i * n + j) * 2 + 1] = z;
@@ -274,7 +297,7 @@ inline cudaError_t ldmd_propagate(double* Y, const double* energies, double mu, 
   cudaError_t err = ldmd_qmid(sec, L, status, stream);
   if (err != cudaSuccess) return err;
   const long long nl = L.is_complex ? L.np / 2 : L.np;
-  const dim3 grid(grid_for(nl * nl, 256, 8192), L.n_energy);
+  const dim3 grid((unsigned)nl, L.n_energy);
   const long long mstride = (long long)L.np * L.np;
   for (int s = 0; s < sec.n_sector; ++s) {
     ldmd_elementwise_kernel<<<grid, 256, 0, stream>>>(s == 0 ? 0 : 1, s, sec, L, Y, Y);

@@ -119,13 +119,16 @@ def propagate_logD(Y_initial, total_energies, reduced_mass: float, radial_half_s
         logger.error(message)
         raise ValueError(message)
     halves = nat.as_device(radial_half_steps, dev, torch.float64)
-    Ws = nat.as_device(W_base_start, dev, torch.float64)
-    Wm = nat.as_device(W_base_mid, dev, torch.float64)
-    We = nat.as_device(W_base_end, dev, torch.float64)
+    # the kernels take W_base exactly symmetric; caller-supplied matrices are symmetrised
+    Ws, Wm, We = (_symmetrised(nat.as_device(W, dev, torch.float64)) for W in (W_base_start, W_base_mid, W_base_end))
     for s0 in range(0, n_sector, MAX_SECTORS_PER_CALL):
         s1 = min(n_sector, s0 + MAX_SECTORS_PER_CALL)
         propagate_device(Y, energies, reduced_mass, halves[s0:s1], Ws[s0:s1], Wm[s0:s1], We[s0:s1])
     return Y
+
+
+def _symmetrised(W: torch.Tensor) -> torch.Tensor:
+    return (0.5 * (W + W.transpose(-1, -2))).contiguous()
 
 
 def propagate_logD_sector(Ymat, radial_half_step: float, W_start, W_mid, W_end, *, device=None) -> torch.Tensor:

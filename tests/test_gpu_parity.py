@@ -258,3 +258,16 @@ def test_mixed_precision_matches_reference(name):
         n = s.shape[0]
         if n:
             assert np.abs(s - g["Smat"][e, :n, :n]).max() <= MIXED_TOL
+
+
+def test_assembled_W_base_is_exactly_symmetric():
+    """The LDMD kernels read W_base[i][j] only; the device assembly must be symmetric bit for bit."""
+    from pyticc_b200 import scattering
+    from pyticc_b200.propagation import runner
+
+    for wl in (workloads.rigid_atom_diatom(jmax=8, J=4, n_energy=2), workloads.morse_atom_diatom(J=8, jmax=10, vmax=1, n_dvr=16, n_theta=12, boundaries=(2.5, 6.0), n_energy=2)):
+        ham = scattering.hamiltonian_for(wl.system, wl.grid)
+        for closed_first in (False, True):
+            dh = runner.device_hamiltonian(ham, nat.require_cuda(), closed_first=closed_first)
+            W = dh.W_base(wl.grid.radial_points[:7])
+            assert torch.equal(W, W.transpose(-1, -2))
