@@ -120,6 +120,29 @@ __device__ __forceinline__ void acc_to_smem(const TileAcc& acc, double* Cs, doub
     }
 }
 
+// Cs[row][col] = acc and, with `mirror`, the same value straight from registers to the
+// transposed position Mt[col * ld + row] (8 lanes of a column write 64 contiguous bytes).
+__device__ __forceinline__ void acc_to_smem_mirror(const TileAcc& acc, double* Cs, double* Mt, long long ld, bool mirror) {
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  const int wm = (warp >> 2) * 64;
+  const int wn = (warp & 3) * 32;
+#pragma unroll
+  for (int mt = 0; mt < 8; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      const int row = wm + mt * 8 + (lane >> 2);
+      const int col = wn + nt * 8 + 2 * (lane & 3);
+      Cs[row * kStride + col] = acc.v[mt][nt][0];
+      Cs[row * kStride + col + 1] = acc.v[mt][nt][1];
+      if (mirror) {
+        Mt[(long long)col * ld + row] = acc.v[mt][nt][0];
+        Mt[(long long)(col + 1) * ld + row] = acc.v[mt][nt][1];
+      }
+    }
+}
+
 // ---- FP32-accurate tile product on the TF32 tensor pipe ---------------------------------
 // The same staged FP64 operands, split on the fly as x = hi + lo with hi, lo TF32
 // (cvt.rna), and D += A_hi B_hi + A_hi B_lo + A_lo B_hi with mma.sync m16n8k8 TF32 and

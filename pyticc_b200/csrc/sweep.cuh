@@ -318,9 +318,10 @@ __global__ void __launch_bounds__(kGemmThreads) sweep_rowpanel_kernel(double* __
   const double* Pt = pinv + (long long)b * 2 * kBlock * kBlock + (kSym ? 0 : kBlock * kBlock);
   TileAcc acc;
   tile_gemm_tn(acc, Pt, kBlock, Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
-  acc_to_smem(acc, smem, 1.0);
+  // U^T into the columns K from registers (symmetric sweep), U rows from shared memory
+  acc_to_smem_mirror(acc, smem, Mb + (long long)c0 * ld + k0, ld, kSym);
   __syncthreads();
-  store_tile(Mb, ld, k0, c0, smem, kSym);
+  store_tile(Mb, ld, k0, c0, smem, false);
   if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) *queue = 0;  // the step's update tile queue
 }
 
