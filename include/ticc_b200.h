@@ -103,6 +103,23 @@ int ticc_ldmd_propagate(void* Y, int is_complex, const double* energies, int n_e
                         long long W_end_stride, int n_sector, int n_channel, int precision, void* workspace, size_t workspace_bytes,
                         int* device_status, void* stream);
 
+/* Several channel blocks through the same sectors in one call: the coupled-states and
+ * NNCC K blocks of one (J, parity) system.  Replaces the per-block loop of
+ * _propagate_blocks (propagation/runner.py:165-322), which calls propagate_logD once per
+ * block and window.  Blocks share n_channel: pad a smaller block with decoupled closed
+ * channels (zero off-diagonal W, a positive W_ii - 2 mu E and a diagonal Y), which leave
+ * the real channels' arithmetic unchanged.
+ *   Y          device, n_block x n_energy x n x n (block-major).
+ *   W_*        block g reads W_*(sector s) at W_* + s * W_*_stride + g * W_block_stride.
+ *   Other arguments as ticc_ldmd_propagate; n_block * n_energy and n_block * n_sector
+ *   must not exceed 65535.  In mixed precision a sweep block is reduced only if it is
+ *   strongly closed in every channel block. */
+int ticc_ldmd_blocks_workspace_size(int n_channel, int n_energy, int n_block, int n_sector, int is_complex, int precision, size_t* bytes);
+int ticc_ldmd_propagate_blocks(void* Y, int is_complex, const double* energies, int n_energy, double reduced_mass, const double* half_steps,
+                               const double* W_start, long long W_start_stride, const double* W_mid, long long W_mid_stride, const double* W_end,
+                               long long W_end_stride, long long W_block_stride, int n_sector, int n_channel, int n_block, int precision,
+                               void* workspace, size_t workspace_bytes, int* device_status, void* stream);
+
 /* ---- PotentialGrid contraction and W assembly --------------------------------
  * V_K(R) = norm [(B_r v(R)) B_r^T + (B_i v(R)) B_i^T] per K group, scattered into the
  * (n_R, n_channel, n_channel) block-diagonal V.  Replaces contract_device /

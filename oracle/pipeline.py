@@ -15,8 +15,12 @@ import numpy as np
 from . import contraction, ldmd, matching
 
 
-def propagate(E_int, U, groups, B_real, B_imag, normalization, potential_values, radial_points, half_steps, reduced_mass, energies, mode="inelastic", window=None, sector_range=None):
-    """Y at the last sector end for every energy (runner.py:165-322)."""
+def propagate(E_int, U, groups, B_real, B_imag, normalization, potential_values, radial_points, half_steps, reduced_mass, energies, mode="inelastic", window=None, sector_range=None, channel_indices=None):
+    """Y at the last sector end for every energy (runner.py:165-322).
+
+    With ``channel_indices`` the propagation covers that channel block only (the CS / NNCC
+    block loop of runner.py:165-322 calls propagate_logD per block): ``E_int`` and ``U``
+    are then the block's, and V is contracted over the block's channels."""
     energies = np.asarray(energies, dtype=np.float64)
     n = len(E_int)
     n_sector = len(half_steps)
@@ -26,7 +30,7 @@ def propagate(E_int, U, groups, B_real, B_imag, normalization, potential_values,
     for start in range(first, last, window):
         stop = min(start + window, last)
         points = slice(2 * start, 2 * stop + 1)
-        V = contraction.contract(groups, B_real, B_imag, normalization, potential_values[points], n)
+        V = contraction.contract(groups, B_real, B_imag, normalization, potential_values[points], n, channel_indices)
         W = contraction.assemble_W_base(radial_points[points], U, E_int, reduced_mass, V)
         if Y is None:
             W0 = W[0][None] - 2.0 * reduced_mass * energies[:, None, None] * np.eye(n)
@@ -35,9 +39,10 @@ def propagate(E_int, U, groups, B_real, B_imag, normalization, potential_values,
     return Y
 
 
-def solve(E_int, U, groups, B_real, B_imag, normalization, potential_values, radial_points, half_steps, reduced_mass, energies, Bmat, L, mode="inelastic", window=None):
-    """Propagate then transform and match (solver.py:142-150, finalize.py:32-98)."""
-    Y = propagate(E_int, U, groups, B_real, B_imag, normalization, potential_values, radial_points, half_steps, reduced_mass, energies, mode, window)
+def solve(E_int, U, groups, B_real, B_imag, normalization, potential_values, radial_points, half_steps, reduced_mass, energies, Bmat, L, mode="inelastic", window=None, channel_indices=None):
+    """Propagate then transform and match (solver.py:142-150, finalize.py:32-98; for one
+    CS / NNCC block, finalize.py:168-225 with the block's Bmat and L)."""
+    Y = propagate(E_int, U, groups, B_real, B_imag, normalization, potential_values, radial_points, half_steps, reduced_mass, energies, mode, window, channel_indices=channel_indices)
     Y_sf = matching.transform_bf_to_sf(Y, Bmat)
     Rmatch = float(radial_points[-1])
     return Y, matching.get_Smat(Y_sf, Rmatch, energies, reduced_mass, E_int, L)

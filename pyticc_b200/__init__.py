@@ -12,15 +12,18 @@ from .energy import get_Etot
 from .match import get_Bmat_BF_to_SF, get_Smat, modified_bessel_K_logD, riccati_bessel_jy, transform_logD_BF_to_SF
 from .pes import PESWrapper
 from .propagation import Propagation, build_radial_sectors, propagate_logD
-from .result import ScatteringResult, Timing
-from .scattering import PotentialGrid, ScattHamiltonian, prepare_potential, solve
+from .kblock import KBlock, build_cs_blocks, build_nncc_blocks
+from .result import CoupledStatesResult, KBlockResult, ScatteringResult, Timing
+from .scattering import PotentialGrid, ScattHamiltonian, build_k_blocks, finalize_K_block, prepare_potential, solve
 from .system import Approx, ChannelSpec, ScatteringType, ScattSystem, build_ScattSystem, reduced_mass
 
 __all__ = [
     "AMU2AU", "AU2CM", "AU2K", "CM2AU", "K2AU",
-    "Approx", "AtomSpec", "Channel", "ChannelBasis", "ChannelSpec", "DiatomBasis", "DiatomSpec", "PESWrapper", "PotentialGrid",
+    "Approx", "AtomSpec", "Channel", "ChannelBasis", "ChannelSpec", "CoupledStatesResult", "DiatomBasis", "DiatomSpec", "KBlock", "KBlockResult",
+    "PESWrapper", "PotentialGrid",
     "Propagation", "RovibBasis", "ScattHamiltonian", "ScattSystem", "ScatteringResult", "ScatteringType", "Timing",
-    "build_ChannelBasis", "build_RovibDVR", "build_ScattSystem", "build_SineDVR", "build_radial_sectors", "get_Bmat_BF_to_SF",
+    "build_ChannelBasis", "build_RovibDVR", "build_ScattSystem", "build_SineDVR", "build_cs_blocks", "build_k_blocks", "build_nncc_blocks",
+    "build_radial_sectors", "finalize_K_block", "get_Bmat_BF_to_SF",
     "get_Etot", "get_Smat", "get_Umat_BF", "modified_bessel_K_logD", "prepare_potential", "propagate_logD", "reduced_mass",
     "riccati_bessel_jy", "solve", "transform_logD_BF_to_SF",
 ]

@@ -45,20 +45,22 @@ struct Carver {
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
-size_t ldmd_layout(ticc::LdmdLayout& L, int n, int n_energy, int n_sector, int is_complex, int precision, char* base) {
+size_t ldmd_layout(ticc::LdmdLayout& L, int n, int n_energy, int n_block, int n_sector, int is_complex, int precision, char* base) {
   Carver c{base};
+  const size_t batch = (size_t)n_block * n_energy;
   L.n = n;
   L.n_energy = n_energy;
+  L.n_block = n_block;
   L.is_complex = is_complex;
   L.np = ticc::ldmd_np(n, is_complex);
   L.npr = ticc::ldmd_np(n, 0);
-  L.M = c.take<double>((size_t)n_energy * L.np * L.np);
-  L.Qm = c.take<double>((size_t)n_sector * L.npr * L.npr);
-  L.y1 = c.take<double>((size_t)n_sector * n_energy * n);
-  L.y2 = c.take<double>((size_t)n_sector * n_energy * n);
+  L.M = c.take<double>(batch * L.np * L.np);
+  L.Qm = c.take<double>((size_t)n_sector * n_block * L.npr * L.npr);
+  L.y1 = c.take<double>((size_t)n_sector * batch * n);
+  L.y2 = c.take<double>((size_t)n_sector * batch * n);
   // one scratch region serves the per-energy sweeps and the per-sector Q_mid sweeps
   // (the latter are chunked to fit); at least one sector's worth is guaranteed
-  const size_t need_e = (size_t)n_energy * ticc::sweep_scratch_doubles(L.np);
+  const size_t need_e = batch * ticc::sweep_scratch_doubles(L.np);
   const size_t need_s = ticc::sweep_scratch_doubles(L.npr) * (size_t)(n_sector < 8 ? n_sector : 8);
   L.scratch_doubles = need_e > need_s ? need_e : need_s;
   L.scratch = c.take<double>(L.scratch_doubles);
@@ -187,31 +189,65 @@ int ticc_sym_inverse(void* M, int n, int batch, int is_complex, void* workspace,
 }
 
 // ---- LDMD propagation ----------------------------------------------------------------------
-int ticc_ldmd_workspace_size(int n_channel, int n_energy, int n_sector, int is_complex, int precision, size_t* bytes) {
-  if (n_channel < 1 || n_energy < 1 || n_sector < 1 || bytes == nullptr)
-    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_ldmd_workspace_size: n_channel=%d n_energy=%d n_sector=%d", n_channel, n_energy, n_sector);
-  if (precision != TICC_PRECISION_FP64 && precision != TICC_PRECISION_MIXED) return fail(TICC_ERR_UNSUPPORTED, "ticc_ldmd_workspace_size: precision mode %d is not available", precision);
+static int ldmd_check_sizes(const char* who, int n_channel, int n_energy, int n_block, int n_sector, int precision) {
+  if (n_channel < 1 || n_energy < 1 || n_block < 1 || n_sector < 1)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "%s: n_channel=%d n_energy=%d n_block=%d n_sector=%d must be positive", who, n_channel, n_energy, n_block, n_sector);
+  if ((long long)n_block * n_energy > 65535 || (long long)n_block * n_sector > 65535)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "%s: n_block*n_energy=%lld and n_block*n_sector=%lld must not exceed 65535 per call", who, (long long)n_block * n_energy,
+                (long long)n_block * n_sector);
+  if (precision != TICC_PRECISION_FP64 && precision != TICC_PRECISION_MIXED) return fail(TICC_ERR_UNSUPPORTED, "%s: precision mode %d is not available", who, precision);
+  return TICC_OK;
+}
+
+static int ldmd_run(const char* who, void* Y, int is_complex, const double* energies, int n_energy, double reduced_mass, const double* half_steps,
+                    const double* W_start, long long W_start_stride, const double* W_mid, long long W_mid_stride, const double* W_end, long long W_end_stride,
+                    long long W_block_stride, int n_sector, int n_channel, int n_block, int precision, void* workspace, size_t workspace_bytes, int* device_status,
+                    void* stream) {
+  if (Y == nullptr || energies == nullptr || half_steps == nullptr || W_start == nullptr || W_mid == nullptr || W_end == nullptr)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "%s: null input pointer", who);
+  const int rc = ldmd_check_sizes(who, n_channel, n_energy, n_block, n_sector, precision);
+  if (rc != TICC_OK) return rc;
+  if (!(reduced_mass > 0.0)) return fail(TICC_ERR_INVALID_ARGUMENT, "%s: reduced_mass must be positive, got %g", who, reduced_mass);
   ticc::LdmdLayout L{};
-  *bytes = ldmd_layout(L, n_channel, n_energy, n_sector, is_complex, precision, nullptr);
+  const size_t need = ldmd_layout(L, n_channel, n_energy, n_block, n_sector, is_complex, precision, nullptr);
+  if (workspace == nullptr || workspace_bytes < need) return fail(TICC_ERR_WORKSPACE, "%s: workspace of %zu bytes given, %zu needed", who, workspace_bytes, need);
+  ldmd_layout(L, n_channel, n_energy, n_block, n_sector, is_complex, precision, static_cast<char*>(workspace));
+  ticc::LdmdSectors sec{half_steps, W_start, W_mid, W_end, W_start_stride, W_mid_stride, W_end_stride, n_sector, W_block_stride};
+  cudaError_t e = ticc::ldmd_propagate(static_cast<double*>(Y), energies, reduced_mass, sec, L, device_status, as_stream(stream));
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, who);
+}
+
+int ticc_ldmd_workspace_size(int n_channel, int n_energy, int n_sector, int is_complex, int precision, size_t* bytes) {
+  if (bytes == nullptr) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_ldmd_workspace_size: null output pointer");
+  const int rc = ldmd_check_sizes("ticc_ldmd_workspace_size", n_channel, n_energy, 1, n_sector, precision);
+  if (rc != TICC_OK) return rc;
+  ticc::LdmdLayout L{};
+  *bytes = ldmd_layout(L, n_channel, n_energy, 1, n_sector, is_complex, precision, nullptr);
   return TICC_OK;
 }
 
 int ticc_ldmd_propagate(void* Y, int is_complex, const double* energies, int n_energy, double reduced_mass, const double* half_steps, const double* W_start,
                         long long W_start_stride, const double* W_mid, long long W_mid_stride, const double* W_end, long long W_end_stride, int n_sector,
                         int n_channel, int precision, void* workspace, size_t workspace_bytes, int* device_status, void* stream) {
-  if (Y == nullptr || energies == nullptr || half_steps == nullptr || W_start == nullptr || W_mid == nullptr || W_end == nullptr)
-    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_ldmd_propagate: null input pointer");
-  if (n_channel < 1 || n_energy < 1 || n_sector < 1)
-    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_ldmd_propagate: n_channel=%d n_energy=%d n_sector=%d must be positive", n_channel, n_energy, n_sector);
-  if (!(reduced_mass > 0.0)) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_ldmd_propagate: reduced_mass must be positive, got %g", reduced_mass);
-  if (precision != TICC_PRECISION_FP64 && precision != TICC_PRECISION_MIXED) return fail(TICC_ERR_UNSUPPORTED, "ticc_ldmd_propagate: precision mode %d is not available", precision);
+  return ldmd_run("ticc_ldmd_propagate", Y, is_complex, energies, n_energy, reduced_mass, half_steps, W_start, W_start_stride, W_mid, W_mid_stride, W_end,
+                  W_end_stride, 0, n_sector, n_channel, 1, precision, workspace, workspace_bytes, device_status, stream);
+}
+
+int ticc_ldmd_blocks_workspace_size(int n_channel, int n_energy, int n_block, int n_sector, int is_complex, int precision, size_t* bytes) {
+  if (bytes == nullptr) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_ldmd_blocks_workspace_size: null output pointer");
+  const int rc = ldmd_check_sizes("ticc_ldmd_blocks_workspace_size", n_channel, n_energy, n_block, n_sector, precision);
+  if (rc != TICC_OK) return rc;
   ticc::LdmdLayout L{};
-  const size_t need = ldmd_layout(L, n_channel, n_energy, n_sector, is_complex, precision, nullptr);
-  if (workspace == nullptr || workspace_bytes < need) return fail(TICC_ERR_WORKSPACE, "ticc_ldmd_propagate: workspace of %zu bytes given, %zu needed", workspace_bytes, need);
-  ldmd_layout(L, n_channel, n_energy, n_sector, is_complex, precision, static_cast<char*>(workspace));
-  ticc::LdmdSectors sec{half_steps, W_start, W_mid, W_end, W_start_stride, W_mid_stride, W_end_stride, n_sector};
-  cudaError_t e = ticc::ldmd_propagate(static_cast<double*>(Y), energies, reduced_mass, sec, L, device_status, as_stream(stream));
-  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_ldmd_propagate");
+  *bytes = ldmd_layout(L, n_channel, n_energy, n_block, n_sector, is_complex, precision, nullptr);
+  return TICC_OK;
+}
+
+int ticc_ldmd_propagate_blocks(void* Y, int is_complex, const double* energies, int n_energy, double reduced_mass, const double* half_steps,
+                               const double* W_start, long long W_start_stride, const double* W_mid, long long W_mid_stride, const double* W_end,
+                               long long W_end_stride, long long W_block_stride, int n_sector, int n_channel, int n_block, int precision, void* workspace,
+                               size_t workspace_bytes, int* device_status, void* stream) {
+  return ldmd_run("ticc_ldmd_propagate_blocks", Y, is_complex, energies, n_energy, reduced_mass, half_steps, W_start, W_start_stride, W_mid, W_mid_stride,
+                  W_end, W_end_stride, W_block_stride, n_sector, n_channel, n_block, precision, workspace, workspace_bytes, device_status, stream);
 }
 
 // ---- contraction ---------------------------------------------------------------------------------

@@ -9,6 +9,11 @@
 //   Y_end = Q_end + y1 - y2 (Y_mid + Q_mid + y1)^{-1} y2
 // The sweep returns S = -A^{-1}, so "- y2 A^{-1} y2" is "+ y2 S y2": every step
 // between two inversions is one fused elementwise pass over the work matrices.
+//
+// Several channel blocks of one size (the K blocks of a coupled-states or NNCC system,
+// padded to a common n) propagate together: the batch is (block g, energy e) with
+// b = g * n_energy + e, block g reads its W at offset g * wb_stride, and Q_mid is one
+// energy-shared matrix per (sector, block).
 #pragma once
 
 #include "sweep.cuh"
@@ -23,17 +28,19 @@ struct LdmdSectors {
   const double* We;
   long long ws_stride, wm_stride, we_stride;
   int n_sector;
+  long long wb_stride;    // offset between the W of consecutive channel blocks (0: one block)
 };
 
 struct LdmdLayout {
   int n;          // logical channels
   int n_energy;
+  int n_block;    // channel blocks; the batch of work matrices is n_block * n_energy
   int is_complex;
   int np;         // padded sweep size of the per-energy work matrix
   int npr;        // padded sweep size of the real, energy-shared Q_mid matrix
-  double* M;      // [n_energy][np][np]
-  double* Qm;     // [n_sector][npr][npr]
-  double* y1;     // [n_sector][n_energy][n]
+  double* M;      // [n_block * n_energy][np][np]
+  double* Qm;     // [n_sector][n_block][npr][npr]
+  double* y1;     // [n_sector][n_block * n_energy][n]
   double* y2;
   double* scratch;
   size_t scratch_doubles;
@@ -63,15 +70,17 @@ __device__ __forceinline__ void reference_pair(double h, double p2, double& y1, 
   }
 }
 
-// y1/y2 for every (sector, energy, channel).
-__global__ void ldmd_reference_kernel(LdmdSectors sec, const double* energies, double mu, int n, int n_energy, double* y1, double* y2) {
-  const long long total = (long long)sec.n_sector * n_energy * n;
+// y1/y2 for every (sector, block, energy, channel).
+__global__ void ldmd_reference_kernel(LdmdSectors sec, const double* energies, double mu, int n, int n_energy, int n_block, double* y1, double* y2) {
+  const long long total = (long long)sec.n_sector * n_block * n_energy * n;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total; idx += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(idx % n);
-    const long long se = idx / n;
-    const int e = (int)(se % n_energy);
-    const int s = (int)(se / n_energy);
-    const double ref = sec.Wm[s * sec.wm_stride + (long long)i * n + i];
+    const long long sb = idx / n;
+    const int e = (int)(sb % n_energy);
+    const long long sg = sb / n_energy;
+    const int g = (int)(sg % n_block);
+    const int s = (int)(sg / n_block);
+    const double ref = sec.Wm[s * sec.wm_stride + g * sec.wb_stride + (long long)i * n + i];
     double a, b;
     reference_pair(sec.h[s], ref - 2.0 * mu * energies[e], a, b);
     y1[idx] = a;
@@ -82,8 +91,9 @@ __global__ void ldmd_reference_kernel(LdmdSectors sec, const double* energies, d
 __device__ __forceinline__ double sym(const double* W, int n, int i, int j) { return 0.5 * (W[(long long)i * n + j] + W[(long long)j * n + i]); }
 
 // Number of leading 128-blocks of the (closed-first ordered) work matrix whose channels
-// are all closed beyond kMixedKappa at the highest energy; one CTA per sector.
-__global__ void ldmd_reduced_blocks_kernel(LdmdSectors sec, const double* energies, double mu, int n, int n_energy, int np, int is_complex, int* reduced) {
+// are all closed beyond kMixedKappa at the highest energy, in every channel block; one CTA
+// per sector.
+__global__ void ldmd_reduced_blocks_kernel(LdmdSectors sec, const double* energies, double mu, int n, int n_energy, int n_block, int np, int is_complex, int* reduced) {
   __shared__ double e_max;
   __shared__ int first_open;
   const int s = blockIdx.x;
@@ -94,10 +104,12 @@ __global__ void ldmd_reduced_blocks_kernel(LdmdSectors sec, const double* energi
     first_open = n;
   }
   __syncthreads();
-  const double* Wm = sec.Wm + s * sec.wm_stride;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const double p2 = Wm[(long long)i * n + i] - 2.0 * mu * e_max;
-    if (!(p2 > kMixedKappa * kMixedKappa)) atomicMin(&first_open, i);
+  for (int g = 0; g < n_block; ++g) {
+    const double* Wm = sec.Wm + s * sec.wm_stride + g * sec.wb_stride;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const double p2 = Wm[(long long)i * n + i] - 2.0 * mu * e_max;
+      if (!(p2 > kMixedKappa * kMixedKappa)) atomicMin(&first_open, i);
+    }
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -106,12 +118,14 @@ __global__ void ldmd_reduced_blocks_kernel(LdmdSectors sec, const double* energi
   }
 }
 
-// Mq = I - h^2 (W_mid - diag ref)/6 (padded identity), batched over sectors.
-__global__ void ldmd_qmid_build_kernel(LdmdSectors sec, int n, int npr, double* Qm) {
-  const int s = blockIdx.y;
+// Mq = I - h^2 (W_mid - diag ref)/6 (padded identity), batched over (sector, block):
+// blockIdx.y = s * n_block + g.
+__global__ void ldmd_qmid_build_kernel(LdmdSectors sec, int n, int n_block, int npr, double* Qm) {
+  const int sg = blockIdx.y;
+  const int s = sg / n_block, g = sg % n_block;
   const double h = sec.h[s];
-  const double* Wm = sec.Wm + s * sec.wm_stride;
-  double* Q = Qm + (long long)s * npr * npr;
+  const double* Wm = sec.Wm + s * sec.wm_stride + g * sec.wb_stride;
+  double* Q = Qm + (long long)sg * npr * npr;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < (long long)npr * npr; idx += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(idx / npr), j = (int)(idx % npr);
     double v;
@@ -125,10 +139,10 @@ __global__ void ldmd_qmid_build_kernel(LdmdSectors sec, int n, int npr, double* 
 }
 
 // Q_mid = (4/h)(X - I) from the swept matrix -X.
-__global__ void ldmd_qmid_finish_kernel(LdmdSectors sec, int n, int npr, double* Qm) {
-  const int s = blockIdx.y;
-  const double h = sec.h[s];
-  double* Q = Qm + (long long)s * npr * npr;
+__global__ void ldmd_qmid_finish_kernel(LdmdSectors sec, int n, int n_block, int npr, double* Qm) {
+  const int sg = blockIdx.y;
+  const double h = sec.h[sg / n_block];
+  double* Q = Qm + (long long)sg * npr * npr;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < (long long)npr * npr; idx += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(idx / npr), j = (int)(idx % npr);
     Q[idx] = (i < n && j < n) ? 4.0 / h * (-Q[idx] - (i == j ? 1.0 : 0.0)) : 0.0;
@@ -168,11 +182,14 @@ __device__ __forceinline__ void put_padding(double* Mb, int np, long long r, lon
 // phase 1: A = [Q_end' + y1' + y2' S y2'] + Q_start + y1   (S from the previous sector)
 // phase 2: B = 2 Q_mid + 2 y1 + y2 S y2
 // phase 3: Y_out = Q_end + y1 + y2 S y2     (last sector of the call)
-// One CTA per (logical row i, energy): the row's reference values are read once, the
-// threads run along j (coalesced M, W and y2 accesses, no per-element index division).
+// One CTA per (logical row i, batch item b = block * n_energy + energy): the row's
+// reference values are read once, the threads run along j (coalesced M, W and y2
+// accesses, no per-element index division).
 __global__ void __launch_bounds__(256) ldmd_elementwise_kernel(int phase, int s, LdmdSectors sec, LdmdLayout L, const double* Yin, double* Yout) {
   const int i = blockIdx.x;
-  const int e = blockIdx.y;
+  const int e = blockIdx.y;  // batch item
+  const int g = e / L.n_energy;
+  const int batch = L.n_block * L.n_energy;
   const int n = L.n, np = L.np;
   const int nl = L.is_complex ? np / 2 : np;  // logical-element grid covering the padded matrix
   double* Mb = L.M + (long long)e * np * np;
@@ -189,11 +206,12 @@ __global__ void __launch_bounds__(256) ldmd_elementwise_kernel(int phase, int s,
     return;
   }
   const double h = sec.h[s];
-  const double* y1 = L.y1 + ((long long)s * L.n_energy + e) * n;
-  const double* y2 = L.y2 + ((long long)s * L.n_energy + e) * n;
-  const double* Ws = sec.Ws + s * sec.ws_stride + (long long)i * n;
-  const double* Wm = sec.Wm + s * sec.wm_stride;
-  const double* We = sec.We + s * sec.we_stride + (long long)i * n;
+  const long long wb = g * sec.wb_stride;
+  const double* y1 = L.y1 + ((long long)s * batch + e) * n;
+  const double* y2 = L.y2 + ((long long)s * batch + e) * n;
+  const double* Ws = sec.Ws + s * sec.ws_stride + wb + (long long)i * n;
+  const double* Wm = sec.Wm + s * sec.wm_stride + wb;
+  const double* We = sec.We + s * sec.we_stride + wb + (long long)i * n;
   const double ref = Wm[(long long)i * n + i];
   const double y1i = y1[i], y2i = y2[i];
   // previous sector (phase 1)
@@ -202,14 +220,14 @@ __global__ void __launch_bounds__(256) ldmd_elementwise_kernel(int phase, int s,
   const double* y2p = nullptr;
   if (phase == 1) {
     hp = sec.h[s - 1];
-    Wep = sec.We + (s - 1) * sec.we_stride + (long long)i * n;
-    const double* y1p = L.y1 + ((long long)(s - 1) * L.n_energy + e) * n;
-    y2p = L.y2 + ((long long)(s - 1) * L.n_energy + e) * n;
-    ref_p = sec.Wm[(s - 1) * sec.wm_stride + (long long)i * n + i];
+    Wep = sec.We + (s - 1) * sec.we_stride + wb + (long long)i * n;
+    const double* y1p = L.y1 + ((long long)(s - 1) * batch + e) * n;
+    y2p = L.y2 + ((long long)(s - 1) * batch + e) * n;
+    ref_p = sec.Wm[(s - 1) * sec.wm_stride + wb + (long long)i * n + i];
     y1pi = y1p[i];
     y2pi = y2p[i];
   }
-  const double* Qrow = L.Qm + (long long)s * L.npr * L.npr + (long long)i * L.npr;
+  const double* Qrow = L.Qm + ((long long)s * L.n_block + g) * L.npr * L.npr + (long long)i * L.npr;
   for (int j = threadIdx.x; j < nl; j += blockDim.x) {
     if (j >= n) {  // padding column
       if (phase == 3) continue;
@@ -268,45 +286,47 @@ inline unsigned grid_for(long long work, int threads, unsigned cap = 1u << 16) {
   return (unsigned)(blocks > cap ? cap : blocks);
 }
 
-// Q_mid for every sector of the call (batched sweep over sectors, chunked to fit scratch).
+// Q_mid for every (sector, block) of the call (batched sweep, chunked to fit scratch).
 inline cudaError_t ldmd_qmid(const LdmdSectors& sec, LdmdLayout& L, int* status, cudaStream_t stream) {
   const long long per = (long long)L.npr * L.npr;
-  ldmd_qmid_build_kernel<<<dim3(grid_for(per, 256, 4096), sec.n_sector), 256, 0, stream>>>(sec, L.n, L.npr, L.Qm);
+  const int count = sec.n_sector * L.n_block;
+  ldmd_qmid_build_kernel<<<dim3(grid_for(per, 256, 4096), count), 256, 0, stream>>>(sec, L.n, L.n_block, L.npr, L.Qm);
   note_launch();
   const int chunk = (int)(L.scratch_doubles / sweep_scratch_doubles(L.npr));
-  for (int s0 = 0; s0 < sec.n_sector; s0 += chunk) {
-    const int cnt = (sec.n_sector - s0 < chunk) ? sec.n_sector - s0 : chunk;
+  for (int s0 = 0; s0 < count; s0 += chunk) {
+    const int cnt = (count - s0 < chunk) ? count - s0 : chunk;
     cudaError_t e = sweep_sym(L.Qm + (long long)s0 * per, per, L.npr, cnt, L.scratch, status, stream);
     if (e != cudaSuccess) return e;
   }
-  ldmd_qmid_finish_kernel<<<dim3(grid_for(per, 256, 4096), sec.n_sector), 256, 0, stream>>>(sec, L.n, L.npr, L.Qm);
+  ldmd_qmid_finish_kernel<<<dim3(grid_for(per, 256, 4096), count), 256, 0, stream>>>(sec, L.n, L.n_block, L.npr, L.Qm);
   note_launch();
   return cudaGetLastError();
 }
 
-// Propagate every energy through every sector of the call.  Y (device, n_energy x n x n,
-// complex interleaved when is_complex) is read at the first sector start and
-// overwritten with the log-derivative at the last sector end.
+// Propagate every (block, energy) through every sector of the call.  Y (device,
+// n_block x n_energy x n x n, complex interleaved when is_complex) is read at the first
+// sector start and overwritten with the log-derivative at the last sector end.
 inline cudaError_t ldmd_propagate(double* Y, const double* energies, double mu, const LdmdSectors& sec, LdmdLayout& L, int* status, cudaStream_t stream) {
-  ldmd_reference_kernel<<<grid_for((long long)sec.n_sector * L.n_energy * L.n, 256), 256, 0, stream>>>(sec, energies, mu, L.n, L.n_energy, L.y1, L.y2);
+  const int batch = L.n_block * L.n_energy;
+  ldmd_reference_kernel<<<grid_for((long long)sec.n_sector * batch * L.n, 256), 256, 0, stream>>>(sec, energies, mu, L.n, L.n_energy, L.n_block, L.y1, L.y2);
   note_launch();
   if (L.reduced != nullptr) {
-    ldmd_reduced_blocks_kernel<<<sec.n_sector, 256, 0, stream>>>(sec, energies, mu, L.n, L.n_energy, L.np, L.is_complex, L.reduced);
+    ldmd_reduced_blocks_kernel<<<sec.n_sector, 256, 0, stream>>>(sec, energies, mu, L.n, L.n_energy, L.n_block, L.np, L.is_complex, L.reduced);
     note_launch();
   }
   cudaError_t err = ldmd_qmid(sec, L, status, stream);
   if (err != cudaSuccess) return err;
   const long long nl = L.is_complex ? L.np / 2 : L.np;
-  const dim3 grid((unsigned)nl, L.n_energy);
+  const dim3 grid((unsigned)nl, batch);
   const long long mstride = (long long)L.np * L.np;
   for (int s = 0; s < sec.n_sector; ++s) {
     ldmd_elementwise_kernel<<<grid, 256, 0, stream>>>(s == 0 ? 0 : 1, s, sec, L, Y, Y);
     note_launch();
-    err = sweep_sym(L.M, mstride, L.np, L.n_energy, L.scratch, status, stream, L.reduced ? L.reduced + s : nullptr);
+    err = sweep_sym(L.M, mstride, L.np, batch, L.scratch, status, stream, L.reduced ? L.reduced + s : nullptr);
     if (err != cudaSuccess) return err;
     ldmd_elementwise_kernel<<<grid, 256, 0, stream>>>(2, s, sec, L, Y, Y);
     note_launch();
-    err = sweep_sym(L.M, mstride, L.np, L.n_energy, L.scratch, status, stream, L.reduced ? L.reduced + s : nullptr);
+    err = sweep_sym(L.M, mstride, L.np, batch, L.scratch, status, stream, L.reduced ? L.reduced + s : nullptr);
     if (err != cudaSuccess) return err;
   }
   ldmd_elementwise_kernel<<<grid, 256, 0, stream>>>(3, sec.n_sector - 1, sec, L, Y, Y);

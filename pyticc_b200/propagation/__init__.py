@@ -3,7 +3,7 @@
 from .config import Propagation, PropagationMode, resolve_device
 from .grid import RadialSector, build_radial_sectors, iter_radial_windows
 from .logd import initialize_logD_capture, initialize_logD_inelastic, propagate_logD, propagate_logD_sector
-from .runner import propagate
+from .runner import propagate, propagate_blocks
 
 __all__ = [
     "Propagation",
@@ -14,6 +14,7 @@ __all__ = [
     "initialize_logD_inelastic",
     "iter_radial_windows",
     "propagate",
+    "propagate_blocks",
     "propagate_logD",
     "propagate_logD_sector",
     "resolve_device",

@@ -85,6 +85,31 @@ def propagate_device(Y: torch.Tensor, energies: torch.Tensor, reduced_mass: floa
     return Y
 
 
+def propagate_blocks_device(Y: torch.Tensor, energies: torch.Tensor, reduced_mass: float, half_steps: torch.Tensor, W_start: torch.Tensor, W_mid: torch.Tensor, W_end: torch.Tensor, *, stride, block_stride: int, precision: int = nat.PRECISION_FP64) -> torch.Tensor:
+    """Propagate device-resident Y of shape (n_block, n_energy, n, n) in place: block g
+    reads its W at element offset g * block_stride from the three W views, whose
+    consecutive sectors are ``stride`` elements apart."""
+    lib = nat.load_library()
+    n_block, n_energy, n, _ = Y.shape
+    n_sector = half_steps.numel()
+    is_complex = int(Y.is_complex())
+    dev = Y.device
+    with torch.cuda.device(dev):
+        nbytes = nat.size_query(lib.ticc_ldmd_blocks_workspace_size, n, n_energy, n_block, n_sector, is_complex, precision)
+        work = nat.Workspace.get(dev, nbytes)
+        status = nat.DeviceStatus(dev)
+        nat.check(
+            lib.ticc_ldmd_propagate_blocks(
+                nat.ptr(Y), is_complex, nat.ptr(energies), n_energy, float(reduced_mass), nat.ptr(half_steps),
+                nat.ptr(W_start), stride[0], nat.ptr(W_mid), stride[1], nat.ptr(W_end), stride[2], int(block_stride),
+                n_sector, n, n_block, precision, nat.ptr(work), work.numel(), status.pointer, nat.stream_handle(dev),
+            ),
+            "ticc_ldmd_propagate_blocks",
+        )
+        status.raise_if_failed("ticc_ldmd_propagate_blocks")
+    return Y
+
+
 def propagate_logD(Y_initial, total_energies, reduced_mass: float, radial_half_steps, W_base_start, W_base_mid, W_base_end, *, device=None) -> torch.Tensor:
     """All energies through all LDMD sectors (logd.py:340-398).
 

@@ -22,7 +22,7 @@ from ..energy import get_Etot
 from ..matrix.interaction import contract_rows, device_rows
 from .config import Propagation, resolve_device
 from .grid import MAX_SECTORS_PER_WINDOW, RadialSector, radial_points_of
-from .logd import propagate_device
+from .logd import propagate_blocks_device, propagate_device
 
 WINDOW_BYTES = 6 * 1024**3  # device budget for one window's W points and Q_mid
 
@@ -145,3 +145,147 @@ def propagate(hamiltonian, Etot, radial_sectors: Sequence[RadialSector], config:
     if dh.position is not None:
         Y = Y[:, dh.position][:, :, dh.position].contiguous()
     return Y
+
+
+# ---- several channel blocks (coupled states, NNCC) -------------------------------------------
+DUMMY_P2 = 3600.0  # local wavenumber^2 (bohr^-2) of the closed channels that pad a smaller block
+
+
+class DeviceBlocks:
+    """Device-resident pieces of several channel blocks of one Hamiltonian, padded to the
+    largest block size n: per block its rows (output positions inside the block), its
+    centrifugal matrix U and thresholds E_int.  Padding channels have no coupling, U = 0
+    and a threshold set per call far above the highest energy, so they stay closed and
+    decoupled.  With ``closed_first`` each block's channels are ordered most-closed first
+    (by W_ii at the outermost grid point), as for one exact-CC block."""
+
+    def __init__(self, hamiltonian, blocks: tuple[tuple[int, ...], ...], device: torch.device, closed_first: bool = False) -> None:
+        self.grid = hamiltonian.potential_grid
+        self.values = self.grid.device_values(device)
+        self.reduced_mass = hamiltonian.reduced_mass
+        self.sizes = tuple(len(b) for b in blocks)
+        self.n = max(self.sizes)
+        self.rows, self.U, self.E_int, self.position = [], [], [], []
+        outer = self.grid.radial_points[-1:]
+        for block in blocks:
+            indices = np.asarray(block, dtype=np.int64)
+            U = np.asarray(hamiltonian.centrifugal(block))
+            E_int = np.asarray(hamiltonian.E_int)[indices]
+            order = np.arange(indices.size)
+            if closed_first:
+                rows = device_rows(hamiltonian.V_basis, device, block)
+                W = self._contract(rows, outer, torch.as_tensor(U, device=device), torch.as_tensor(E_int, device=device))[0]
+                order = np.argsort(-torch.diagonal(W).cpu().numpy(), kind="stable")
+            rows = device_rows(hamiltonian.V_basis, device, tuple(int(c) for c in indices[order]))
+            rows.n_channel = self.n
+            U_pad = np.zeros((self.n, self.n))
+            U_pad[: order.size, : order.size] = U[np.ix_(order, order)]
+            position = np.empty_like(order)
+            position[order] = np.arange(order.size)
+            self.rows.append(rows)
+            self.U.append(torch.as_tensor(U_pad, device=device))
+            self.E_int.append(E_int[order])
+            self.position.append(torch.as_tensor(position, device=device))
+
+    def _contract(self, rows, radial_points, U, E_int, out=None):
+        dev = U.device
+        index = torch.as_tensor(self.grid.selection(radial_points), device=dev)
+        potential = self.values.index_select(0, index)
+        R = torch.as_tensor(np.ascontiguousarray(radial_points), device=dev)
+        return contract_rows(rows, potential, radial_points=R, U=U, E_int=E_int, reduced_mass=self.reduced_mass, out=out)
+
+    def thresholds(self, energies: np.ndarray, device: torch.device) -> list[torch.Tensor]:
+        """Per block E_int padded with the closed padding thresholds for these energies."""
+        dummy = float(np.max(energies)) + DUMMY_P2 / (2.0 * self.reduced_mass)
+        out = []
+        for E_int in self.E_int:
+            padded = np.full(self.n, dummy)
+            padded[: E_int.size] = E_int
+            out.append(torch.as_tensor(padded, device=device))
+        return out
+
+    def W_base(self, g: int, radial_points: np.ndarray, E_int: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+        return self._contract(self.rows[g], radial_points, self.U[g], E_int, out=out)
+
+
+_DEVICE_BLOCKS: dict = {}
+
+
+def device_blocks(hamiltonian, blocks, device: torch.device, closed_first: bool = False) -> DeviceBlocks:
+    key = (id(hamiltonian), blocks, device.index, closed_first)
+    cached = _DEVICE_BLOCKS.get(key)
+    if cached is None:
+        cached = DeviceBlocks(hamiltonian, blocks, device, closed_first)
+        _DEVICE_BLOCKS[key] = cached
+    return cached
+
+
+def blocks_window(n_channel: int, n_block: int, n_sector: int) -> int:
+    """Sectors per window so that every block's W points and Q_mid fit the window budget."""
+    padded = -(-n_channel // 128) * 128
+    per_sector = 8 * n_block * (2 * n_channel * n_channel + padded * padded)
+    return max(1, min(n_sector, MAX_SECTORS_PER_WINDOW, WINDOW_BYTES // per_sector, 65535 // n_block))
+
+
+def propagate_blocks(hamiltonian, channel_blocks, Etot, radial_sectors: Sequence[RadialSector], config: Propagation, *, window_timing: list | None = None) -> tuple[torch.Tensor, ...]:
+    """Y at the last sector end of every channel block, one (n_energy, n_b, n_b) device
+    tensor per block (reference runner.py:165-322).  All blocks share each radial window
+    and advance together in one batched LDMD call per window."""
+    energies_np = get_Etot(Etot)
+    blocks = tuple(tuple(int(i) for i in b) for b in channel_blocks)
+    if not blocks or any(not b for b in blocks):
+        message = "At least one non-empty channel block is required for propagation"
+        logger.error(message)
+        raise ValueError(message)
+    if not radial_sectors:
+        message = "Propagation produced no radial windows"
+        logger.error(message)
+        raise RuntimeError(message)
+    dev = resolve_device(config.device)
+    mixed = config.precision == "mixed"
+    db = device_blocks(hamiltonian, blocks, dev, closed_first=mixed)
+    n, n_block = db.n, len(blocks)
+    energies = torch.as_tensor(np.array(energies_np), device=dev)
+    E_pad = db.thresholds(energies_np, dev)
+    n_sector = len(radial_sectors)
+    size = blocks_window(n, n_block, n_sector)
+    precision = nat.PRECISION_MIXED if mixed else nat.PRECISION_FP64
+    logger.info(f"Propagation device: gpu:{dev.index}, x64=True")
+    if config.print_verbose:
+        logger.info(f"Propagation started: blocks={n_block}, sectors={n_sector}, channels={max(db.sizes)}, energies={energies_np.size}, pes_prefetch=False")
+    started = perf_counter()
+    interval = max(1, ceil(n_sector / 10))
+    next_report = interval
+    points_max = 2 * size + 1
+    W = torch.empty((n_block, points_max, n, n), dtype=torch.float64, device=dev)
+    Y = None
+    done = 0
+    flops_per_unit = sum(2.0 * float(m) ** 3 for m in db.sizes)
+    for s0 in range(0, n_sector, size):
+        window = tuple(radial_sectors[s0 : s0 + size])
+        points = radial_points_of(window)
+        for g in range(n_block):
+            db.W_base(g, points, E_pad[g], W[g, : points.size])
+        if Y is None:
+            Y = torch.stack([initial_logD(W[g, 0], energies, db.reduced_mass, config.mode) for g in range(n_block)]).contiguous()
+        halves = torch.as_tensor(np.asarray([s.radial_half_step for s in window]), device=dev)
+        stride = 2 * n * n
+        if window_timing is not None:
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record()
+        propagate_blocks_device(Y, energies, db.reduced_mass, halves, W[0, 0], W[0, 1], W[0, 2], stride=(stride, stride, stride), block_stride=points_max * n * n, precision=precision)
+        if window_timing is not None:
+            t1.record()
+            window_timing.append((t0, t1, flops_per_unit * len(window) * energies.numel()))
+        done += len(window)
+        if config.print_verbose and (done == n_sector or done >= next_report):
+            torch.cuda.synchronize(dev)
+            logger.info(f"Propagation: {done}/{n_sector} sectors, R={window[-1].radial_end:.6f} bohr, wall={perf_counter() - started:.3f} s")
+            while next_report <= done:
+                next_report += interval
+    out = []
+    for g, size_g in enumerate(db.sizes):
+        pos = db.position[g]
+        out.append(Y[g, :, :size_g, :size_g][:, pos][:, :, pos].contiguous())
+    return tuple(out)
+

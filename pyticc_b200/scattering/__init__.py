@@ -24,8 +24,9 @@ from ..matrix.interaction import DeviceBasisCache, VBasisBF, contract_device, pr
 from ..pes import PESWrapper, get_Vgrid_atom_diatom, get_Vgrid_diatom_diatom
 from ..propagation.config import Propagation
 from ..propagation.grid import RadialSector, build_radial_sectors, radial_points_of
-from ..result import ScatteringResult, Timing
-from ..system import ScatteringType, ScattSystem
+from ..kblock import KBlock, build_cs_blocks, build_nncc_blocks
+from ..result import CoupledStatesResult, KBlockResult, ScatteringResult, Timing
+from ..system import Approx, ScatteringType, ScattSystem
 
 
 @dataclass(frozen=True, slots=True)
@@ -149,11 +150,25 @@ class ScattHamiltonian:
     reduced_mass: float
     V_basis: VBasisBF
     potential_grid: PotentialGrid
+    approx: Approx = Approx.EXACT
+    K_delta: int = 1
     _device_cache: DeviceBasisCache = field(default_factory=DeviceBasisCache, compare=False, repr=False)
+
+    def __post_init__(self) -> None:
+        if self.K_delta < 1:
+            message = f"K_delta must be positive, but got {self.K_delta}"
+            logger.error(message)
+            raise ValueError(message)
 
     @property
     def E_int(self) -> np.ndarray:
         return self.basis.E_int
+
+    def centrifugal(self, channel_indices: Sequence[int] | None = None) -> np.ndarray:
+        """U over the selected channels in the given order (hamiltonian.py:87-110): the
+        field-free BF matrix keeps the K -> K+1 Coriolis couplings inside the selection, so
+        a single-K (CS) block has none and an NNCC window keeps those between its K."""
+        return get_Umat_BF(self.basis, channel_indices)
 
     @property
     def U(self) -> np.ndarray:
@@ -188,7 +203,7 @@ def build_hamiltonian(system: ScattSystem, potential_grid: PotentialGrid) -> Sca
             system.basis, system.monomer_X.rovib, system.monomer_Y.rovib,
             g.coordinate("cos_theta_X"), g.weight("theta_X"), g.coordinate("cos_theta_Y"), g.weight("theta_Y"), g.coordinate("phi"), g.weight("phi"),
         )
-    return ScattHamiltonian(system.basis, float(system.reduced_mass), vb, potential_grid)
+    return ScattHamiltonian(system.basis, float(system.reduced_mass), vb, potential_grid, system.approx, system.K_delta)
 
 
 _HAMILTONIANS: dict[tuple[int, int], ScattHamiltonian] = {}
@@ -204,12 +219,45 @@ def hamiltonian_for(system: ScattSystem, potential_grid: PotentialGrid) -> Scatt
     return cached
 
 
-def solve(problem: ScattSystem, Etot, potential_grid: PotentialGrid, propagation: Propagation, *, sectors: Sequence[RadialSector] | None = None) -> ScatteringResult:
-    """Build (or reuse), propagate and match one exact-CC block (reference solver.py:57-178).
+def build_k_blocks(hamiltonian: ScattHamiltonian) -> tuple[KBlock, ...]:
+    """CS or NNCC propagation blocks of one Hamiltonian (solver.py:203-216)."""
+    if hamiltonian.approx is Approx.CS:
+        return build_cs_blocks(hamiltonian.basis)
+    if hamiltonian.approx is Approx.NNCC:
+        return build_nncc_blocks(hamiltonian.basis, hamiltonian.K_delta)
+    message = f"Coupled-states blocks require approx='cs' or 'nncc', but got {hamiltonian.approx.value!r}"
+    logger.error(message)
+    raise ValueError(message)
+
+
+def _match(Y: torch.Tensor, B: np.ndarray, L: np.ndarray, E_int: np.ndarray, Rmatch: float, energies: np.ndarray, reduced_mass: float) -> tuple[np.ndarray, ...]:
+    """BF -> SF transform and matching on the device; one open-open S per energy."""
+    Y_sf = transform_device(Y, nat.as_device(B, Y.device, torch.float64))
+    S, n_open = get_Smat_device(Y_sf, Rmatch, energies, reduced_mass, E_int, L)
+    S_host = S.cpu().numpy()
+    return tuple(np.ascontiguousarray(S_host[e, : n_open[e], : n_open[e]]) for e in range(energies.size))
+
+
+def finalize_K_block(basis, block: KBlock, Y_BF: torch.Tensor, Etot, reduced_mass: float, Rmatch: float, *, approx: Approx = Approx.NNCC) -> KBlockResult:
+    """Transform, match and package one CS or NNCC block (finalize.py:168-225); ``Y_BF`` is
+    the block's device log-derivative batch (n_energy, n_b, n_b)."""
+    energies = get_Etot(Etot)
+    indices = np.asarray(block.channel_indices, dtype=np.int64)
+    E_int = basis.E_int[indices]
+    B, L = get_Bmat_BF_to_SF(basis, block.channel_indices)
+    smats = _match(Y_BF, B, L, E_int, Rmatch, energies, reduced_mass)
+    open_indices = tuple(indices[np.flatnonzero(E_int < e)] for e in energies)
+    return KBlockResult(block, open_indices, Y_BF.cpu().numpy(), B, L, smats)
+
+
+def solve(problem: ScattSystem, Etot, potential_grid: PotentialGrid, propagation: Propagation, *, sectors: Sequence[RadialSector] | None = None) -> ScatteringResult | CoupledStatesResult:
+    """Build (or reuse), propagate and match one (J, parity) system (reference
+    solver.py:57-178): exact CC returns a ScatteringResult; CS and NNCC propagate their K
+    blocks together and return a CoupledStatesResult.
 
     ``sectors`` optionally replaces the grid's fixed-step sectors by another schedule whose
     start/mid/end points all lie on the grid (e.g. a learned step schedule)."""
-    from ..propagation.runner import propagate
+    from ..propagation.runner import propagate, propagate_blocks
 
     if not isinstance(problem, ScattSystem):
         message = "solve requires a ScattSystem"
@@ -222,23 +270,35 @@ def solve(problem: ScattSystem, Etot, potential_grid: PotentialGrid, propagation
     energies = get_Etot(Etot)
     wall, cpu = perf_counter(), process_time()
     basis = problem.basis
-    logger.info(f"Solving Jtot={basis.Jtot}, system_parity={basis.system_parity:+d}, approx=exact, channels={basis.n_channel}, energies={energies.size}")
+    logger.info(f"Solving Jtot={basis.Jtot}, system_parity={basis.system_parity:+d}, approx={problem.approx.value}, channels={basis.n_channel}, energies={energies.size}")
     if basis.n_channel == 0:
         message = "At least one non-empty channel block is required for propagation"
         logger.error(message)
         raise ValueError(message)
     hamiltonian = hamiltonian_for(problem, potential_grid)
     run_sectors = potential_grid.sectors if sectors is None else tuple(sectors)
+    if problem.approx is not Approx.EXACT:
+        if sectors is None and propagation.steps == "learned":
+            message = "Learned sector widths are trained for exact coupled channels; use steps='fixed' with CS/NNCC"
+            logger.error(message)
+            raise ValueError(message)
+        blocks = build_k_blocks(hamiltonian)
+        Y_blocks = propagate_blocks(hamiltonian, tuple(b.channel_indices for b in blocks), energies, run_sectors, propagation)
+        Rmatch = run_sectors[-1].radial_end
+        results = tuple(
+            finalize_K_block(basis, block, Y_b, energies, hamiltonian.reduced_mass, Rmatch, approx=problem.approx)
+            for block, Y_b in zip(blocks, Y_blocks, strict=True)
+        )
+        timing = Timing(perf_counter() - wall, process_time() - cpu)
+        logger.info(f"Solver complete: {timing}")
+        return CoupledStatesResult(basis, energies, problem.approx, results, timing)
     if sectors is None and propagation.steps == "learned":
         from ..propagation.learned import learned_sectors, resolve_proposer
 
         run_sectors = learned_sectors(hamiltonian, run_sectors, energies, resolve_proposer(propagation.proposer), propagation.device)
     Y = propagate(hamiltonian, energies, run_sectors, propagation)
     B, L = get_Bmat_BF_to_SF(basis)
-    Y_sf = transform_device(Y, nat.as_device(B, Y.device, torch.float64))
-    S, n_open = get_Smat_device(Y_sf, run_sectors[-1].radial_end, energies, hamiltonian.reduced_mass, basis.E_int, L)
-    S_host = S.cpu().numpy()
-    smats = tuple(np.ascontiguousarray(S_host[e, : n_open[e], : n_open[e]]) for e in range(energies.size))
+    smats = _match(Y, B, L, basis.E_int, run_sectors[-1].radial_end, energies, hamiltonian.reduced_mass)
     timing = Timing(perf_counter() - wall, process_time() - cpu)
     logger.info(f"Solver complete: {timing}")
     return ScatteringResult(basis, energies, Y.cpu().numpy(), B, L, smats, timing)

@@ -82,6 +82,7 @@ class ScattSystem:
     approx: Approx = Approx.EXACT
     scattering_type: ScatteringType | None = None
     basis: object = None
+    K_delta: int = 1
 
     def __post_init__(self) -> None:
         if self.system_parity not in (-1, 1):
@@ -90,6 +91,10 @@ class ScattSystem:
             raise ValueError(message)
         if self.Jtot < 0:
             message = f"Jtot must be non-negative, but got {self.Jtot}"
+            logger.error(message)
+            raise ValueError(message)
+        if self.K_delta < 1:
+            message = f"Invalid K_delta {self.K_delta}. Must be positive."
             logger.error(message)
             raise ValueError(message)
 
@@ -117,22 +122,26 @@ def build_ScattSystem(
     system_parity: int,
     channel: ChannelSpec | None = None,
     approx: Approx = Approx.EXACT,
+    K_delta: int = 1,
     potential=None,
     reduced_mass: float | None = None,
 ) -> ScattSystem:
-    """Build a system and its channel basis (reference ``system.py:466-777``, field-free branch)."""
+    """Build a system and its channel basis (reference ``system.py:466-777``, field-free branch).
+
+    ``approx`` selects exact coupled channels, coupled states (one block per K) or NNCC
+    (overlapping windows of 2 K_delta + 1 helicities)."""
     from .basis import build_ChannelBasis
 
-    if approx is not Approx.EXACT:
-        message = "Only exact coupled channels are built by this library; CS/NNCC blocks are not on its path"
+    if not isinstance(approx, Approx):
+        message = f"approx must be an Approx, but got {approx!r}"
         logger.error(message)
-        raise NotImplementedError(message)
+        raise TypeError(message)
     if reduced_mass is not None and (not np.isfinite(reduced_mass) or reduced_mass <= 0.0):
         message = f"reduced_mass must be positive, but got {reduced_mass}"
         logger.error(message)
         raise ValueError(message)
     spec = ChannelSpec() if channel is None else channel
-    system = ScattSystem(monomer_X, monomer_Y, Jtot, system_parity, potential, reduced_mass, spec, approx, _infer_type(monomer_X, monomer_Y))
+    system = ScattSystem(monomer_X, monomer_Y, Jtot, system_parity, potential, reduced_mass, spec, approx, _infer_type(monomer_X, monomer_Y), K_delta=K_delta)
     return replace(system, basis=build_ChannelBasis(monomer_X, monomer_Y, Jtot, system_parity, spec))
 
 

@@ -16,7 +16,7 @@ from .basis import AtomSpec, DiatomBasis, RovibBasis, build_RovibDVR, build_Sine
 from .constants import AMU2AU, CM2AU, K2AU
 from .pes import PESWrapper
 from .scattering import PotentialGrid, prepare_potential
-from .system import ScattSystem, build_ScattSystem
+from .system import Approx, ScattSystem, build_ScattSystem
 
 
 def rigid_rotor(B_cm: float, jmax: int) -> DiatomBasis:
@@ -104,37 +104,37 @@ class Workload:
     mode: str = "inelastic"
 
 
-def rigid_atom_diatom(*, B_cm=20.0, jmax=20, J=20, parity=1, mu_amu=18.0, eps_cm=150.0, Rm=6.5, a1=0.3, a2=0.2, n_theta=24, boundaries=(2.5, 30.0), half_steps=(0.05,), energies_cm=None, n_energy=16) -> Workload:
+def rigid_atom_diatom(*, B_cm=20.0, jmax=20, J=20, parity=1, mu_amu=18.0, eps_cm=150.0, Rm=6.5, a1=0.3, a2=0.2, n_theta=24, boundaries=(2.5, 30.0), half_steps=(0.05,), energies_cm=None, n_energy=16, approx=Approx.EXACT, K_delta=1) -> Workload:
     """Plain A+BC rigid rotor (the CPU-runnable configuration at full size)."""
     energies = np.linspace(10.0, 500.0, n_energy) * CM2AU if energies_cm is None else np.asarray(energies_cm) * CM2AU
-    system = build_ScattSystem(AtomSpec(), rigid_rotor(B_cm, jmax), Jtot=J, system_parity=parity, potential=lj_aniso_pes(eps_cm, Rm, a1, a2), reduced_mass=mu_amu * AMU2AU)
+    system = build_ScattSystem(AtomSpec(), rigid_rotor(B_cm, jmax), Jtot=J, system_parity=parity, potential=lj_aniso_pes(eps_cm, Rm, a1, a2), reduced_mass=mu_amu * AMU2AU, approx=approx, K_delta=K_delta)
     return Workload("rigid_atom_diatom", system, prepare_potential(system, boundaries, half_steps, n_theta=n_theta), energies)
 
 
 MORSE_DEFAULTS = dict(De_cm=40000.0, re=1.4, a=1.2, mass_amu=1.0, r_interval=(0.5, 3.5), n_dvr=32, vmax=3, jmax=30)
 
 
-def morse_atom_diatom(*, J=30, parity=1, mu_amu=18.0, eps_cm=150.0, Rm=6.5, a1=0.3, a2=0.2, seed=2024, n_theta=32, boundaries=(2.5, 40.0), half_steps=(0.02,), energies_cm=None, n_energy=256, diatom=None, **diatom_args) -> Workload:
+def morse_atom_diatom(*, J=30, parity=1, mu_amu=18.0, eps_cm=150.0, Rm=6.5, a1=0.3, a2=0.2, seed=2024, n_theta=32, boundaries=(2.5, 40.0), half_steps=(0.02,), energies_cm=None, n_energy=256, diatom=None, approx=Approx.EXACT, K_delta=1, **diatom_args) -> Workload:
     """Vibrating A+BC: Morse diatom (v <= 3, j <= 30) with r-dependent anisotropy c_k ~ U(-1/2, 1/2)."""
     params = {**MORSE_DEFAULTS, **diatom_args}
     c1, c2 = np.random.default_rng(seed).uniform(-0.5, 0.5, size=2)
     diatom = morse_diatom(**params) if diatom is None else diatom
     energies = np.linspace(100.0, 3000.0, n_energy) * CM2AU if energies_cm is None else np.asarray(energies_cm) * CM2AU
-    system = build_ScattSystem(AtomSpec(), diatom, Jtot=J, system_parity=parity, potential=lj_aniso_pes(eps_cm, Rm, a1, a2, c1, c2, params["re"]), reduced_mass=mu_amu * AMU2AU)
+    system = build_ScattSystem(AtomSpec(), diatom, Jtot=J, system_parity=parity, potential=lj_aniso_pes(eps_cm, Rm, a1, a2, c1, c2, params["re"]), reduced_mass=mu_amu * AMU2AU, approx=approx, K_delta=K_delta)
     return Workload("morse_atom_diatom", system, prepare_potential(system, boundaries, half_steps, n_theta=n_theta), energies)
 
 
-def rotor_pair(*, B1_cm=60.0, B2_cm=2.0, jmax=8, J=6, parity=1, mu_amu=3.6, lmax=4, seed=11, strength_cm=40.0, lj_eps_cm=100.0, lj_Rm=6.0, n_theta_X=15, n_theta_Y=15, n_phi=12, boundaries=(2.5, 30.0), half_steps=(0.05,), energies_cm=None, n_energy=128) -> Workload:
+def rotor_pair(*, B1_cm=60.0, B2_cm=2.0, jmax=8, J=6, parity=1, mu_amu=3.6, lmax=4, seed=11, strength_cm=40.0, lj_eps_cm=100.0, lj_Rm=6.0, n_theta_X=15, n_theta_Y=15, n_phi=12, boundaries=(2.5, 30.0), half_steps=(0.05,), energies_cm=None, n_energy=128, approx=Approx.EXACT, K_delta=1) -> Workload:
     """AB+CD rigid rotors with a seeded bispherical expansion plus isotropic LJ."""
     terms = bispherical_terms(lmax, seed)
     energies = np.linspace(5.0, 800.0, n_energy) * CM2AU if energies_cm is None else np.asarray(energies_cm) * CM2AU
-    system = build_ScattSystem(rigid_rotor(B1_cm, jmax), rigid_rotor(B2_cm, jmax), Jtot=J, system_parity=parity, potential=bispherical_pes(terms, strength_cm, lj_eps_cm, lj_Rm), reduced_mass=mu_amu * AMU2AU)
+    system = build_ScattSystem(rigid_rotor(B1_cm, jmax), rigid_rotor(B2_cm, jmax), Jtot=J, system_parity=parity, potential=bispherical_pes(terms, strength_cm, lj_eps_cm, lj_Rm), reduced_mass=mu_amu * AMU2AU, approx=approx, K_delta=K_delta)
     grid = prepare_potential(system, boundaries, half_steps, n_theta_X=n_theta_X, n_theta_Y=n_theta_Y, n_phi=n_phi)
     return Workload("rotor_pair", system, grid, energies)
 
 
-def ultracold_capture(*, B_cm=0.03, jmax=40, J=10, parity=1, mu_amu=100.0, C6=1.0e4, wall_cm=500.0, seed=3, n_theta=48, boundaries=(8.0, 1500.0), half_steps=(0.05,), energies_K=None, n_energy=512) -> Workload:
+def ultracold_capture(*, B_cm=0.03, jmax=40, J=10, parity=1, mu_amu=100.0, C6=1.0e4, wall_cm=500.0, seed=3, n_theta=48, boundaries=(8.0, 1500.0), half_steps=(0.05,), energies_K=None, n_energy=512, approx=Approx.EXACT, K_delta=1) -> Workload:
     """Capture-mode A+BC: ultracold energies log-uniform over 1 uK .. 1 mK."""
     energies = np.geomspace(1.0e-6, 1.0e-3, n_energy) * K2AU if energies_K is None else np.asarray(energies_K) * K2AU
-    system = build_ScattSystem(AtomSpec(), rigid_rotor(B_cm, jmax), Jtot=J, system_parity=parity, potential=capture_pes(C6, wall_cm, seed), reduced_mass=mu_amu * AMU2AU)
+    system = build_ScattSystem(AtomSpec(), rigid_rotor(B_cm, jmax), Jtot=J, system_parity=parity, potential=capture_pes(C6, wall_cm, seed), reduced_mass=mu_amu * AMU2AU, approx=approx, K_delta=K_delta)
     return Workload("ultracold_capture", system, prepare_potential(system, boundaries, half_steps, n_theta=n_theta), energies, mode="capture")

@@ -4,7 +4,7 @@ Run once in a container that has the reference checked out (JAX itself is not
 needed: ``tests/golden/_jaxshim`` is a NumPy-backed stand-in for the few JAX calls
 the reference makes)::
 
-    python tests/golden/make_golden.py /path/to/PyTICC/src
+    python tests/golden/make_golden.py /path/to/PyTICC/src [fixture names...]
 
 Every fixture is a small ``.npz`` written next to this script.  The product never
 reads these files; ``tests/`` uses them to pin the oracle and the CUDA path.
@@ -416,13 +416,143 @@ def make_channel_counts() -> None:
     _save("channel_counts", counts)
 
 
+def make_kblocks() -> None:
+    """CS and NNCC block structures from the reference's own block builders."""
+    from pyticc.basis.channel import build_ChannelBasis
+    from pyticc.basis.kblock import build_cs_blocks, build_nncc_blocks
+    from pyticc.basis.monomer import DiatomSpec
+
+    cases = {
+        "atom_j4_J4": (ticc.AtomSpec(), DiatomSpec(Eint=np.zeros((1, 5))), 4, 1, None),
+        "atom_j6_J9_p-": (ticc.AtomSpec(), DiatomSpec(Eint=np.zeros((2, 7))), 9, -1, None),
+        "atom_j8_J8_Kcut3": (ticc.AtomSpec(), DiatomSpec(Eint=np.zeros((1, 9))), 8, 1, 3),
+        "pair_j3_J5": (DiatomSpec(Eint=np.zeros((1, 4))), DiatomSpec(Eint=np.zeros((1, 3))), 5, 1, None),
+        "atom_j2_J0": (ticc.AtomSpec(), DiatomSpec(Eint=np.zeros((1, 3))), 0, 1, None),
+    }
+    table = {}
+    for name, (X, Y, J, parity, K_cut) in cases.items():
+        system = ticc.ScattSystem(X, Y, Jtot=J, system_parity=parity)
+        channels = build_ChannelBasis(system, ticc.ChannelSpec(K_cut=K_cut))
+        entry = {"K": [float(c.K) for c in channels], "cs": [], "nncc": {}}
+        for block in build_cs_blocks(channels):
+            entry["cs"].append([list(block.K_values), list(block.channel_indices), list(block.owned_K_values), list(block.owned_channel_indices), block.center_K])
+        for K_delta in (1, 2, 3):
+            entry["nncc"][str(K_delta)] = [
+                [list(b.K_values), list(b.channel_indices), list(b.owned_K_values), list(b.owned_channel_indices), b.center_K]
+                for b in build_nncc_blocks(channels, K_delta=K_delta)
+            ]
+        table[name] = entry
+    _save("kblocks", {"cases": table})
+
+
+def _solve_blocks_and_save(name, params, system, boundaries, halves, energies, mode, **quad):
+    grid = ticc.prepare_potential(system, boundaries, halves, **quad)
+    result = ticc.solve(system, energies, grid, ticc.Propagation(mode=mode, device="cpu"))
+    basis = system.basis
+    payload = {
+        "energies": np.asarray(energies),
+        "n_block": np.asarray(len(result.blocks)),
+        "E_int": basis.E_int,
+        "radial_points": grid.radial_points,
+        "potential_values": np.asarray(grid.values),
+        "half_steps_sectors": np.asarray([s.radial_half_step for s in grid.sectors]),
+        "U": ticc.scattering.ScattHamiltonian(basis=basis, reduced_mass=system.reduced_mass, interaction=lambda R: None).U,
+        **_vbasis_rows(system, grid),
+    }
+    for b, block in enumerate(result.blocks):
+        n = len(block.block.channel_indices)
+        payload[f"b{b}_channel_indices"] = np.asarray(block.block.channel_indices)
+        payload[f"b{b}_owned"] = np.asarray(block.block.owned_channel_indices)
+        payload[f"b{b}_K_values"] = np.asarray(block.block.K_values)
+        payload[f"b{b}_Y_BF"] = np.asarray(block.Y_BF)
+        payload[f"b{b}_Bmat"] = np.asarray(block.Bmat)
+        payload[f"b{b}_L"] = np.asarray(block.L)
+        payload[f"b{b}_Smat"] = _pad_smat(block.Smat_asymptotic, n)
+        payload[f"b{b}_n_open"] = np.asarray([m.shape[0] for m in block.Smat_asymptotic])
+        payload[f"b{b}_Smat_BF"] = _pad_smat(block.Smat_BF, n)
+    _save(name, params, **payload)
+
+
+def make_solve_kblocks() -> None:
+    """CS and NNCC solves of the rigid A+BC, vibrating A+BC and AB+CD fixtures' systems."""
+    rigid = {"B_cm": 20.0, "jmax": 5, "J": 3, "mu_amu": 18.0, "eps_cm": 150.0, "Rm": 6.5, "a1": 0.3, "a2": 0.2, "n_theta": 8, "boundaries": [2.5, 10.0], "half_steps": [0.05]}
+    energies = np.linspace(10.0, 500.0, 5) * CM
+    for approx, K_delta, mode, tag in ((ticc.Approx.CS, 1, "inelastic", "cs"), (ticc.Approx.NNCC, 1, "inelastic", "nncc"), (ticc.Approx.CS, 1, "capture", "cs_capture")):
+        system = ticc.build_ScattSystem(
+            ticc.AtomSpec(),
+            _rigid_rotor(rigid["B_cm"], rigid["jmax"]),
+            Jtot=rigid["J"],
+            system_parity=1,
+            approx=approx,
+            K_delta=K_delta,
+            potential=_lj_aniso_pes(rigid["eps_cm"], rigid["Rm"], rigid["a1"], rigid["a2"]),
+            reduced_mass=rigid["mu_amu"] * AMU,
+        )
+        _solve_blocks_and_save(f"solve_rigid_{tag}", {**rigid, "parity": 1, "approx": approx.value, "K_delta": K_delta, "mode": mode}, system, rigid["boundaries"], rigid["half_steps"], energies, mode, n_theta=rigid["n_theta"])
+    # rotor pair (AB+CD) under NNCC with K_delta = 1 and J = 3 (K = 0..3)
+    pair = {"B1_cm": 60.0, "B2_cm": 2.0, "jmax": 2, "J": 3, "mu_amu": 3.6, "lmax": 2, "seed": 11, "strength_cm": 40.0, "lj_eps_cm": 100.0, "lj_Rm": 6.0, "n_theta_X": 6, "n_theta_Y": 6, "n_phi": 5, "boundaries": [4.0, 10.0], "half_steps": [0.05]}
+    from pyticc.basis.angle import clebsch_gordan, norm_YjK
+
+    rng = np.random.default_rng(pair["seed"])
+    terms = []
+    for l1 in range(pair["lmax"] + 1):
+        for l2 in range(pair["lmax"] + 1):
+            for lam in range(abs(l1 - l2), min(l1 + l2, pair["lmax"]) + 1):
+                if (l1 + l2 + lam) % 2 == 0 and (l1, l2, lam) != (0, 0, 0):
+                    terms.append((l1, l2, lam, float(rng.normal())))
+
+    def interaction(R, coordinates):
+        _, _, t1, t2, phi = coordinates
+        x1, x2 = np.cos(t1), np.cos(t2)
+        total = np.zeros_like(x1)
+        for l1, l2, lam, c in terms:
+            angular = np.zeros_like(x1)
+            for m in range(-min(l1, l2), min(l1, l2) + 1):
+                angular += float(clebsch_gordan(l1, m, l2, -m, lam)) * norm_YjK(l1, m, x1) * norm_YjK(l2, -m, x2) * np.cos(m * phi)
+            total += c * angular
+        radial = pair["strength_cm"] * CM * np.exp(-0.8 * (R - 6.0))
+        lj = pair["lj_eps_cm"] * CM * ((pair["lj_Rm"] / R) ** 12 - 2.0 * (pair["lj_Rm"] / R) ** 6)
+        return radial * total + lj
+
+    system = ticc.build_ScattSystem(
+        _rigid_rotor(pair["B1_cm"], pair["jmax"]),
+        _rigid_rotor(pair["B2_cm"], pair["jmax"]),
+        Jtot=pair["J"],
+        system_parity=1,
+        approx=ticc.Approx.NNCC,
+        K_delta=1,
+        potential=ticc.PESWrapper(interaction=interaction),
+        reduced_mass=pair["mu_amu"] * AMU,
+    )
+    _solve_blocks_and_save(
+        "solve_pair_nncc",
+        {**pair, "terms": terms, "approx": "nncc", "K_delta": 1, "mode": "inelastic"},
+        system,
+        pair["boundaries"],
+        pair["half_steps"],
+        np.array([5.0, 200.0, 800.0]) * CM,
+        "inelastic",
+        n_theta_X=pair["n_theta_X"],
+        n_theta_Y=pair["n_theta_Y"],
+        n_phi=pair["n_phi"],
+    )
+
+
+MAKERS = {
+    "ldmd": make_ldmd,
+    "contract": make_contract,
+    "smatrix": make_smatrix,
+    "bessel": make_bessel,
+    "grid": make_grid,
+    "solve_rigid": make_solve_rigid,
+    "solve_morse": make_solve_morse,
+    "solve_diatom_diatom": make_solve_diatom_diatom,
+    "channel_counts": make_channel_counts,
+    "kblocks": make_kblocks,
+    "solve_kblocks": make_solve_kblocks,
+}
+
 if __name__ == "__main__":
-    make_ldmd()
-    make_contract()
-    make_smatrix()
-    make_bessel()
-    make_grid()
-    make_solve_rigid()
-    make_solve_morse()
-    make_solve_diatom_diatom()
-    make_channel_counts()
+    # python make_golden.py <reference src> [fixture names...]  (default: all)
+    for key in sys.argv[2:] or list(MAKERS):
+        MAKERS[key]()
