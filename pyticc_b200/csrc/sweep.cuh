@@ -223,9 +223,22 @@ __global__ void __launch_bounds__(kPivotThreads) sweep_pivot_kernel(double* __re
   double* aux = smem + kBlock * kPivotLd;
   const int b = blockIdx.x;
   double* Mb = M + (long long)b * mstride;
-  for (int idx = threadIdx.x; idx < kBlock * kBlock; idx += kPivotThreads) {
-    const int r = idx >> 7, c = idx & (kBlock - 1);
-    P[r * kPivotLd + c] = Mb[(long long)(k0 + r) * ld + k0 + c];
+  // 128 x 128 block as double2 pieces, 8 loads in flight per thread
+#pragma unroll 1
+  for (int base = 0; base < kBlock * 64; base += 8 * kPivotThreads) {
+    double2 m[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int piece = base + u * kPivotThreads + threadIdx.x;
+      m[u] = *reinterpret_cast<const double2*>(Mb + (long long)(k0 + (piece >> 6)) * ld + k0 + (piece & 63) * 2);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int piece = base + u * kPivotThreads + threadIdx.x;
+      double* d = P + (piece >> 6) * kPivotLd + (piece & 63) * 2;
+      d[0] = m[u].x;
+      d[1] = m[u].y;
+    }
   }
   __syncthreads();
   invert_pivot_block<kSym>(P, aux, Mb, ld, k0, pinv, b, status);
