@@ -43,6 +43,7 @@ def parse_args():
     p.add_argument("--schedule", choices=["fixed", "learned"], default="learned", help="headline arm sector schedule")
     p.add_argument("--plain-steps", type=int, default=None, help="timed steps of the plain FP64 fixed-step arm (default: steps - 1, at least 1)")
     p.add_argument("--sectors", type=int, default=0, help="limit sectors (0 = all 938); for quick checks only")
+    p.add_argument("--approx", choices=["exact", "cs", "nncc"], default="exact", help="exact CC (the metric) or the coupled-states / NNCC (K_delta=1) blocks of the same system")
     return p.parse_args()
 
 
@@ -97,14 +98,16 @@ class ClockSampler:
 
 
 def build_workload(args):
+    import pyticc_b200 as tb
     from pyticc_b200 import workloads
 
     halves = (0.02,)
     bounds = (2.5, 40.0)
     blocks = []
     diatom = workloads.morse_diatom(**workloads.MORSE_DEFAULTS)
+    approx = tb.Approx(getattr(args, "approx", "exact"))
     for parity in (1, -1):
-        wl = workloads.morse_atom_diatom(parity=parity, diatom=diatom, boundaries=bounds, half_steps=halves, n_energy=256)
+        wl = workloads.morse_atom_diatom(parity=parity, diatom=diatom, boundaries=bounds, half_steps=halves, n_energy=256, approx=approx, K_delta=1)
         blocks.append(wl)
     return blocks
 
@@ -207,6 +210,9 @@ def main():
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.approx != "exact":
+        run_blocks(args, rank, world, local)
         return
     import torch
 
@@ -363,6 +369,127 @@ def main():
             "kernel": "ticc_ldmd_propagate of the headline arm (batched symmetric sweeps; FP64 DMMA, TF32x3 on strongly closed blocks in mixed precision); peak = cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)",
             "flops_per_unit": f"2 N^3 per (sector, energy), N={n_channel}, counted in FP64-equivalent flops",
         },
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_blocks(args, rank, world, local):
+    """Coupled-states or NNCC solves of the benchmark system: every K block of one parity
+    block propagated together (one batched LDMD call per window) and matched per block."""
+    import torch
+
+    import pyticc_b200 as tb
+    from oracle import contraction, ldmd
+    from pyticc_b200 import _native as nat
+    from pyticc_b200 import scattering
+    from pyticc_b200.propagation import runner
+    from pyticc_b200.replicas import max_over_ranks
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    group = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+        group = dist
+    lib = nat.load_library()
+    blocks = build_workload(args)
+    sectors_of = [b.grid.sectors if args.sectors == 0 else b.grid.sectors[: args.sectors] for b in blocks]
+    config = tb.Propagation(precision="fp64")
+    plan = units(blocks, args.batch, rank, world, args.warmup + args.steps)
+    k_blocks = [scattering.build_k_blocks(scattering.hamiltonian_for(b.system, b.grid)) for b in blocks]
+
+    def one_step(block_index, energy_slice, windows=None):
+        wl = blocks[block_index]
+        ham = scattering.hamiltonian_for(wl.system, wl.grid)
+        energies = wl.energies[energy_slice]
+        sectors = sectors_of[block_index]
+        kb = k_blocks[block_index]
+        Ys = runner.propagate_blocks(ham, tuple(b.channel_indices for b in kb), energies, sectors, config, window_timing=windows)
+        return [scattering.finalize_K_block(wl.system.basis, b, Y, energies, ham.reduced_mass, sectors[-1].radial_end, approx=wl.system.approx) for b, Y in zip(kb, Ys, strict=True)]
+
+    for k in range(args.warmup):
+        one_step(*plan[k])
+    torch.cuda.synchronize()
+    if group:
+        group.barrier()
+    launches0 = lib.ticc_kernel_launches()
+    windows: list = []
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record()
+        for k in range(args.warmup, args.warmup + args.steps):
+            one_step(*plan[k], windows)
+        stop.record()
+        torch.cuda.synchronize()
+    launches = lib.ticc_kernel_launches() - launches0
+    elapsed = max_over_ranks(start.elapsed_time(stop) * 1e-3, group)
+    value = args.steps * args.batch * world / elapsed
+    prop_seconds = sum(a.elapsed_time(b) * 1e-3 for a, b, _ in windows)
+    prop_flops = sum(f for _, _, f in windows)
+    peak = fp64_peak_tflops(torch, dev) if rank == 0 else 0.0
+    e2e_value, h2d, d2h, cpu = None, 0, 0, None
+    if rank == 0:
+        wl = blocks[plan[args.warmup][0]]
+        energies = np.ascontiguousarray(wl.energies[plan[args.warmup][1]])
+        wl.grid._device_cache.clear()
+        runner._DEVICE_BLOCKS.clear()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        result = tb.solve(wl.system, energies, wl.grid, config)
+        e2e_seconds = time.perf_counter() - t0
+        e2e_value = len(energies) / e2e_seconds
+        h2d = int(energies.nbytes + wl.grid.values.nbytes)
+        d2h = int(sum(b.Y_BF.nbytes + sum(x.nbytes for x in b.Smat_asymptotic) for b in result.blocks))
+        # oracle: one energy through 4 sectors for every block, extrapolated in sectors
+        ham = scattering.hamiltonian_for(wl.system, wl.grid)
+        U = ham.U
+        pts, n_s = 9, 4
+        values = wl.grid.values.reshape(wl.grid.radial_points.size, -1)[:pts]
+        hs = np.asarray([s.radial_half_step for s in wl.grid.sectors[:n_s]])
+        E = energies[:1]
+        t0 = time.perf_counter()
+        for b in k_blocks[plan[args.warmup][0]]:
+            idx = list(b.channel_indices)
+            V = contraction.contract(ham.V_basis.channel_indices, ham.V_basis.B_real, None, 1.0, values, len(idx), idx)
+            W = contraction.assemble_W_base(wl.grid.radial_points[:pts], U[np.ix_(idx, idx)], wl.system.basis.E_int[idx], wl.system.reduced_mass, V)
+            Y0 = ldmd.initialize_inelastic(W[0][None] - 2 * wl.system.reduced_mass * E[:, None, None] * np.eye(len(idx)))
+            ldmd.propagate_logD(Y0, E, wl.system.reduced_mass, hs, W[0:-1:2], W[1::2], W[2::2])
+        cpu_s = time.perf_counter() - t0
+        cpu = {"value": 1.0 / (cpu_s / n_s * len(wl.grid.sectors)), "unit": "solves/s", "cores": torch.get_num_threads(), "kind": "port",
+               "sample": f"1 energy x {n_s} of {len(wl.grid.sectors)} sectors for all {len(k_blocks[0])} blocks ({cpu_s:.1f} s), extrapolated linearly in sectors; NumPy/LAPACK LDMD restatement of the reference"}
+    if group:
+        group.barrier()
+        group.destroy_process_group()
+    if rank != 0:
+        return
+    sizes = [len(b.channel_indices) for b in k_blocks[0]]
+    achieved = prop_flops / prop_seconds / 1e12 if prop_seconds else None
+    line = {
+        "metric": f"{args.approx.upper()} S-matrix solves/s on 1 B200 (one solve = every K block of one (J, parity) block at one energy)",
+        "value": value,
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": elapsed / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD.replace("exact CC", f"{args.approx.upper()} blocks (K_delta=1)" if args.approx == "nncc" else "CS blocks"), "batch": args.batch,
+                   "blocks": len(sizes), "block_channels": [min(sizes), max(sizes)], "sectors": len(sectors_of[0]), "l2": "inputs larger than L2 (W windows of every block > 1 GiB)"},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if achieved and peak else None, "traffic": None,
+                     "kernel": "ticc_ldmd_propagate_blocks (all K blocks batched; pivot-block inversions dominate for blocks of <= 128 channels)",
+                     "flops_per_unit": "sum over blocks of 2 n_b^3 per (sector, energy)"},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),

@@ -180,7 +180,7 @@ int ticc_sym_inverse(void* M, int n, int batch, int is_complex, void* workspace,
   cudaStream_t s = as_stream(stream);
   sym_load_kernel<<<dim3(ticc::grid_for(nl * nl, 256, 8192), batch), 256, 0, s>>>(static_cast<double*>(M), n, is_complex, Mw, np);
   ticc::note_launch();
-  cudaError_t e = ticc::sweep_sym(Mw, (long long)np * np, np, batch, scratch, device_status, s);
+  cudaError_t e = ticc::sweep_sym(Mw, (long long)np * np, np, batch, scratch, device_status, s, nullptr, is_complex ? 2 * n : n);
   if (e != cudaSuccess) return cuda_fail(e, "ticc_sym_inverse");
   sym_store_kernel<<<dim3(ticc::grid_for((long long)n * n, 256, 8192), batch), 256, 0, s>>>(Mw, np, static_cast<double*>(M), n, is_complex);
   ticc::note_launch();

@@ -295,7 +295,7 @@ inline cudaError_t ldmd_qmid(const LdmdSectors& sec, LdmdLayout& L, int* status,
   const int chunk = (int)(L.scratch_doubles / sweep_scratch_doubles(L.npr));
   for (int s0 = 0; s0 < count; s0 += chunk) {
     const int cnt = (count - s0 < chunk) ? count - s0 : chunk;
-    cudaError_t e = sweep_sym(L.Qm + (long long)s0 * per, per, L.npr, cnt, L.scratch, status, stream);
+    cudaError_t e = sweep_sym(L.Qm + (long long)s0 * per, per, L.npr, cnt, L.scratch, status, stream, nullptr, L.n);
     if (e != cudaSuccess) return e;
   }
   ldmd_qmid_finish_kernel<<<dim3(grid_for(per, 256, 4096), count), 256, 0, stream>>>(sec, L.n, L.n_block, L.npr, L.Qm);
@@ -319,14 +319,15 @@ inline cudaError_t ldmd_propagate(double* Y, const double* energies, double mu, 
   const long long nl = L.is_complex ? L.np / 2 : L.np;
   const dim3 grid((unsigned)nl, batch);
   const long long mstride = (long long)L.np * L.np;
+  const int used = L.is_complex ? 2 * L.n : L.n;  // rows of the work matrix beyond these are identity padding
   for (int s = 0; s < sec.n_sector; ++s) {
     ldmd_elementwise_kernel<<<grid, 256, 0, stream>>>(s == 0 ? 0 : 1, s, sec, L, Y, Y);
     note_launch();
-    err = sweep_sym(L.M, mstride, L.np, batch, L.scratch, status, stream, L.reduced ? L.reduced + s : nullptr);
+    err = sweep_sym(L.M, mstride, L.np, batch, L.scratch, status, stream, L.reduced ? L.reduced + s : nullptr, used);
     if (err != cudaSuccess) return err;
     ldmd_elementwise_kernel<<<grid, 256, 0, stream>>>(2, s, sec, L, Y, Y);
     note_launch();
-    err = sweep_sym(L.M, mstride, L.np, batch, L.scratch, status, stream, L.reduced ? L.reduced + s : nullptr);
+    err = sweep_sym(L.M, mstride, L.np, batch, L.scratch, status, stream, L.reduced ? L.reduced + s : nullptr, used);
     if (err != cudaSuccess) return err;
   }
   ldmd_elementwise_kernel<<<grid, 256, 0, stream>>>(3, sec.n_sector - 1, sec, L, Y, Y);

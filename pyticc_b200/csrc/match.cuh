@@ -190,7 +190,7 @@ inline cudaError_t match_smatrix(const double* Y, double Rmatch, const double* e
   const long long nlz = L.is_complex ? L.npz / 2 : L.npz;
   match_build_z_kernel<<<dim3(grid_for(nlz * nlz, 256, 8192), L.n_energy), 256, 0, stream>>>(L, Y);
   note_launch();
-  cudaError_t err = sweep_sym(L.Z, (long long)L.npz * L.npz, L.npz, L.n_energy, L.scratch, status, stream);
+  cudaError_t err = sweep_sym(L.Z, (long long)L.npz * L.npz, L.npz, L.n_energy, L.scratch, status, stream, nullptr, L.is_complex ? 2 * L.n : L.n);
   if (err != cudaSuccess) return err;
   const long long nla = L.npa / 2;
   match_build_ab_kernel<<<dim3(grid_for(nla * nla, 256, 8192), L.n_energy), 256, 0, stream>>>(L, n_open);

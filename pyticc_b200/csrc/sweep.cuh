@@ -25,17 +25,19 @@ namespace ticc {
 
 constexpr int kPivotLd = kStride;  // the pivot block lives in a [128][kStride] shared tile
 constexpr int kSub = 64;           // Gauss-Jordan sub-block of the pivot block
-constexpr size_t kPivotAuxBytes = size_t(2) * kSub * kSub * sizeof(double) + 2 * kSub * sizeof(double) + 4 * sizeof(double) + (4 + kSub) * sizeof(int);
+constexpr size_t kGJAuxDoubles = 2 * kSub + 4;  // Gauss-Jordan bookkeeping: pivot row, pivot column, candidates
+constexpr size_t kPivotAuxBytes = size_t(2) * kSub * kSub * sizeof(double) + kGJAuxDoubles * sizeof(double) + (4 + kSub) * sizeof(int);
 constexpr size_t kPivotSmemBytes = size_t(kBlock) * kPivotLd * sizeof(double) + kPivotAuxBytes;
 constexpr size_t kUpdateSmemBytes = kUpdTileSmemBytes + 16;  // + the broadcast slot of the tile queue  // stages + C tile; the pivot aux reuses the stages
 static_assert(kPivotAuxBytes <= size_t(kUpdStageDoubles) * sizeof(double), "pivot scratch must fit in the update stages");
 
-// Gauss-Jordan exchange of a 64x64 sub-block S (row stride kPivotLd) with partial
+// Gauss-Jordan exchange of a 64x64 sub-block S (row stride Ld) with partial
 // pivoting over its rows, by the kPivotThreads threads of the CTA; writes the inverse in
 // natural order to X (row stride kSub).  Thread t owns column t % 64 and every 4th row
 // from t / 64, so a step updates 16 elements per thread branch-free, the pivot row and
 // column are broadcast reads and the next pivot search runs in the 4 owners of the next
 // column.  Two barriers per step.  Returns true if a pivot was zero or non-finite.
+template <int Ld = kPivotLd>
 __device__ inline bool gauss_jordan_sub(double* S, double* X, double* aux) {
   constexpr int G = kPivotThreads / kSub;
   constexpr int RPT = kSub / G;
@@ -52,7 +54,8 @@ __device__ inline bool gauss_jordan_sub(double* S, double* X, double* aux) {
     int row = kSub;
 #pragma unroll
     for (int i = 0; i < RPT; ++i) {
-      const double v = fabs(S[(g + G * i) * kPivotLd]);
+      const double m = fabs(S[(g + G * i) * Ld]);
+      const double v = (m >= 0.0) ? m : 0.0;  // a NaN entry ranks as zero, then flags the pivot
       if (v > best) {
         best = v;
         row = g + G * i;
@@ -74,14 +77,14 @@ __device__ inline bool gauss_jordan_sub(double* S, double* X, double* aux) {
         p = r;
       }
     }
-    double a = S[p * kPivotLd + j];
+    double a = S[p * Ld + j];
     if (!(fabs(a) > 0.0) || !isfinite(a)) {
       singular = true;
       a = 1.0;
     }
     const double inv_a = 1.0 / a;
-    if (g == 0) prow[c] = S[p * kPivotLd + c];
-    if (g == G - 1) pcol[c] = S[c * kPivotLd + j];
+    if (g == 0) prow[c] = S[p * Ld + c];
+    if (g == G - 1) pcol[c] = S[c * Ld + j];
     if (t == 0) perm[j] = p;
     if (p % G == g) used |= 1u << (p / G);
     __syncthreads();
@@ -90,7 +93,7 @@ __device__ inline bool gauss_jordan_sub(double* S, double* X, double* aux) {
 #pragma unroll
     for (int u = 0; u < RPT; ++u) pc[u] = pcol[g + G * u];
 #pragma unroll
-    for (int u = 0; u < RPT; ++u) v[u] = S[(g + G * u) * kPivotLd + c];
+    for (int u = 0; u < RPT; ++u) v[u] = S[(g + G * u) * Ld + c];
     const int mine = (p % G == g) ? p / G : -1;
 #pragma unroll
     for (int u = 0; u < RPT; ++u) {
@@ -98,13 +101,14 @@ __device__ inline bool gauss_jordan_sub(double* S, double* X, double* aux) {
       v[u] = (u == mine) ? ((c == j) ? inv_a : -pr) : w;
     }
 #pragma unroll
-    for (int u = 0; u < RPT; ++u) S[(g + G * u) * kPivotLd + c] = v[u];
+    for (int u = 0; u < RPT; ++u) S[(g + G * u) * Ld + c] = v[u];
     if (c == j + 1) {
       double b2 = -1.0;
       int row = kSub;
 #pragma unroll
       for (int u = 0; u < RPT; ++u) {
-        const double w = ((used >> u) & 1u) ? -1.0 : fabs(v[u]);
+        const double m = fabs(v[u]);
+        const double w = ((used >> u) & 1u) ? -1.0 : (m >= 0.0 ? m : 0.0);
         if (w > b2) {
           b2 = w;
           row = g + G * u;
@@ -121,7 +125,7 @@ __device__ inline bool gauss_jordan_sub(double* S, double* X, double* aux) {
   __syncthreads();
   for (int e = t; e < kSub * kSub; e += kPivotThreads) {
     const int jj = e / kSub, m = e % kSub;
-    X[e] = S[perm[jj] * kPivotLd + iperm[m]];
+    X[e] = S[perm[jj] * Ld + iperm[m]];
   }
   __syncthreads();
   return singular;
@@ -242,6 +246,44 @@ __global__ void __launch_bounds__(kPivotThreads) sweep_pivot_kernel(double* __re
   }
   __syncthreads();
   invert_pivot_block<kSym>(P, aux, Mb, ld, k0, pinv, b, status);
+}
+
+// Sweep of a single-block matrix whose channels fill at most the leading 64 rows and
+// columns (the rest is identity padding): only the 64x64 block is inverted, in a CTA with
+// 69 KB of shared memory so that three matrices share an SM; the padding becomes -I.
+constexpr int kSmallLd = kSub + 4;
+constexpr size_t kPivot64SmemBytes = (size_t(kSub) * kSmallLd + size_t(kSub) * kSub + kGJAuxDoubles) * sizeof(double) + (4 + kSub) * sizeof(int);
+template <bool kSym>
+__global__ void __launch_bounds__(kPivotThreads) sweep_pivot64_kernel(double* __restrict__ M, long long mstride, int ld, int* status) {
+  extern __shared__ double smem[];
+  double* S = smem;
+  double* X = S + kSub * kSmallLd;
+  double* gj = X + kSub * kSub;
+  const int b = blockIdx.x;
+  double* Mb = M + (long long)b * mstride;
+#pragma unroll
+  for (int u = 0; u < kSub * kSub / 2 / kPivotThreads; ++u) {
+    const int piece = u * kPivotThreads + threadIdx.x;
+    const double2 m = *reinterpret_cast<const double2*>(Mb + (long long)(piece >> 5) * ld + (piece & 31) * 2);
+    double* d = S + (piece >> 5) * kSmallLd + (piece & 31) * 2;
+    d[0] = m.x;
+    d[1] = m.y;
+  }
+  __syncthreads();
+  const bool singular = gauss_jordan_sub<kSmallLd>(S, X, gj);
+  if (singular && threadIdx.x == 0) report_status(status, kDeviceSingularPivot, b, 0);
+  for (int idx = threadIdx.x; idx < ld * ld; idx += kPivotThreads) {
+    const int i = idx / ld, j = idx % ld;
+    double x;
+    if (i < kSub && j < kSub) {
+      x = X[i * kSub + j];
+      if (kSym) x = 0.5 * (x + X[j * kSub + i]);
+      x = -x;
+    } else {
+      x = (i == j) ? -1.0 : 0.0;
+    }
+    Mb[(long long)i * ld + j] = x;
+  }
 }
 
 // Cs[r][c] += M[r0 + r][c0 + c] for a 128x128 tile; 8 global loads in flight per batch.
@@ -507,6 +549,8 @@ template <bool kSym>
 inline cudaError_t sweep_configure_variant() {
   cudaError_t e = cudaFuncSetAttribute(sweep_pivot_kernel<kSym>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPivotSmemBytes);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(sweep_pivot64_kernel<kSym>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPivot64SmemBytes);
+  if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(sweep_rowpanel_kernel<kSym>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmemBytes);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(sweep_update_kernel<kSym>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmemBytes);
@@ -526,10 +570,15 @@ inline cudaError_t sweep_configure() {
 // Launches: one pivot kernel, then per block a row panel (and column panel for the
 // general sweep) and an update that also inverts the next pivot block.
 template <bool kSym>
-inline cudaError_t sweep_batched(double* M, long long mstride, int np, int batch, double* scratch, int* status, cudaStream_t stream, const int* reduced_blocks = nullptr) {
+inline cudaError_t sweep_batched(double* M, long long mstride, int np, int batch, double* scratch, int* status, cudaStream_t stream, const int* reduced_blocks = nullptr, int n_used = 0) {
   cudaError_t e = sweep_configure();
   if (e != cudaSuccess) return e;
   const int nt = np / kBlock;
+  if (nt == 1 && n_used > 0 && n_used <= kSub) {
+    sweep_pivot64_kernel<kSym><<<batch, kPivotThreads, kPivot64SmemBytes, stream>>>(M, mstride, np, status);
+    note_launch();
+    return cudaGetLastError();
+  }
   const long long cstride = (long long)kBlock * np;
   double* cold = scratch;
   double* pinv = scratch + (long long)batch * cstride;
@@ -564,8 +613,9 @@ inline cudaError_t sweep_batched(double* M, long long mstride, int np, int batch
   return cudaGetLastError();
 }
 
-inline cudaError_t sweep_sym(double* M, long long mstride, int np, int batch, double* scratch, int* status, cudaStream_t stream, const int* reduced_blocks = nullptr) {
-  return sweep_batched<true>(M, mstride, np, batch, scratch, status, stream, reduced_blocks);
+// n_used > 0 states that only the leading n_used rows and columns differ from the identity.
+inline cudaError_t sweep_sym(double* M, long long mstride, int np, int batch, double* scratch, int* status, cudaStream_t stream, const int* reduced_blocks = nullptr, int n_used = 0) {
+  return sweep_batched<true>(M, mstride, np, batch, scratch, status, stream, reduced_blocks, n_used);
 }
 inline cudaError_t sweep_general(double* M, long long mstride, int np, int batch, double* scratch, int* status, cudaStream_t stream) {
   return sweep_batched<false>(M, mstride, np, batch, scratch, status, stream);

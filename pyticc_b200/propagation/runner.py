@@ -241,6 +241,16 @@ def propagate_blocks(hamiltonian, channel_blocks, Etot, radial_sectors: Sequence
         message = "Propagation produced no radial windows"
         logger.error(message)
         raise RuntimeError(message)
+    # blocks that fit the 64-wide single-block sweep (64 real rows, or 32 complex channels)
+    # go in their own batch, so that they are not padded to the larger blocks' size
+    small = 32 if config.mode == "capture" else 64
+    classes = [[g for g, b in enumerate(blocks) if len(b) <= small], [g for g, b in enumerate(blocks) if len(b) > small]]
+    if all(classes):
+        out: list = [None] * len(blocks)
+        for members in classes:
+            for g, Y in zip(members, propagate_blocks(hamiltonian, tuple(blocks[g] for g in members), Etot, radial_sectors, config, window_timing=window_timing), strict=True):
+                out[g] = Y
+        return tuple(out)
     dev = resolve_device(config.device)
     mixed = config.precision == "mixed"
     db = device_blocks(hamiltonian, blocks, dev, closed_first=mixed)
