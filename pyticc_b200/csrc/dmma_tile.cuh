@@ -262,8 +262,14 @@ __device__ __forceinline__ void acc32_to_smem(const TileAcc32& acc, double* Cs, 
 // product.  K-chunks of kUpdChunk rows keep both staging buffers and the C tile resident:
 //   [ A/B stages: 2 x 2 x kUpdChunk x kStride ][ C tile: 128 x kStride ]   (doubles)
 constexpr int kUpdChunk = 16;
-constexpr int kUpdStageDoubles = 2 * 2 * kUpdChunk * kStride;  // 8448 doubles = 67584 B
-constexpr size_t kUpdTileSmemBytes = (size_t(kUpdStageDoubles) + size_t(kBlock) * kStride) * sizeof(double);  // 202752
+// TF32x3 operands split once while staging: per stage A_hi, A_lo, B_hi, B_lo as 32-bit words,
+// kUpdChunk rows of kSplitLd words (136 = 8 mod 32: conflict-free tf32 fragment loads)
+constexpr int kSplitLd = kBlock + 8;
+constexpr int kSplitArray = kUpdChunk * kSplitLd;
+constexpr int kSplitStageWords = 4 * kSplitArray;
+constexpr int kUpdStageDoubles64 = 2 * 2 * kUpdChunk * kStride;  // FP64 stages: 8448 doubles
+constexpr int kUpdStageDoubles = kUpdStageDoubles64 > kSplitStageWords ? kUpdStageDoubles64 : kSplitStageWords;  // 2 split stages = 8704 doubles
+constexpr size_t kUpdTileSmemBytes = (size_t(kUpdStageDoubles) + size_t(kBlock) * kStride) * sizeof(double);  // 204800
 
 __device__ __forceinline__ void mma_chunk_any(TileAcc& acc, const double* As, const double* Bs, int warp, int lane) { mma_chunk<kUpdChunk>(acc, As, Bs, warp, lane); }
 __device__ __forceinline__ void mma_chunk_any(TileAcc32& acc, const double* As, const double* Bs, int warp, int lane) { mma_chunk_tf32x3<kUpdChunk>(acc, As, Bs, warp, lane); }
@@ -393,6 +399,169 @@ __device__ __forceinline__ void acc_sub_smem(const TileAcc32& acc, double* Cs, d
           Mt[(long long)(col + 1) * ld + row] = v1;
         }
       }
+}
+
+// Epilogue written straight from the accumulator registers: M[r0 + row][c0 + col] = C - acc
+// with C from the staged tile Cs (a double2 per lane pair of columns).  An off-diagonal tile
+// of the symmetric sweep also writes its transpose (the 8 lanes sharing a column write 64
+// contiguous bytes); a diagonal tile writes each lower-half value (row >= col) to both of
+// its positions, so the tile stays exactly symmetric.  Cs is only read.
+__device__ __forceinline__ void put_updated(double* Mb, long long ld, int r0, int c0, int row, int col, double v0, double v1, bool sym) {
+  if (!sym || r0 != c0) {
+    *reinterpret_cast<double2*>(Mb + (long long)(r0 + row) * ld + c0 + col) = make_double2(v0, v1);
+    if (sym) {
+      Mb[(long long)(c0 + col) * ld + r0 + row] = v0;
+      Mb[(long long)(c0 + col + 1) * ld + r0 + row] = v1;
+    }
+  } else {
+    if (row >= col) {
+      Mb[(long long)(r0 + row) * ld + c0 + col] = v0;
+      Mb[(long long)(c0 + col) * ld + r0 + row] = v0;
+    }
+    if (row >= col + 1) {
+      Mb[(long long)(r0 + row) * ld + c0 + col + 1] = v1;
+      Mb[(long long)(c0 + col + 1) * ld + r0 + row] = v1;
+    }
+  }
+}
+__device__ __forceinline__ void acc_epilogue_direct(const TileAcc& acc, const double* Cs, double* Mb, long long ld, int r0, int c0, bool sym) {
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  const int wm = (warp >> 2) * 64;
+  const int wn = (warp & 3) * 32;
+#pragma unroll
+  for (int mt = 0; mt < 8; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      const int row = wm + mt * 8 + (lane >> 2), col = wn + nt * 8 + 2 * (lane & 3);
+      const double2 c = *reinterpret_cast<const double2*>(Cs + row * kStride + col);
+      put_updated(Mb, ld, r0, c0, row, col, c.x - acc.v[mt][nt][0], c.y - acc.v[mt][nt][1], sym);
+    }
+}
+__device__ __forceinline__ void acc_epilogue_direct(const TileAcc32& acc, const double* Cs, double* Mb, long long ld, int r0, int c0, bool sym) {
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  const int wm = (warp >> 2) * 64;
+  const int wn = (warp & 3) * 32;
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int row = wm + mt * 16 + g + 8 * h, col = wn + nt * 8 + 2 * t;
+        const double2 c = *reinterpret_cast<const double2*>(Cs + row * kStride + col);
+        put_updated(Mb, ld, r0, c0, row, col, c.x - (double)acc.v[mt][nt][2 * h], c.y - (double)acc.v[mt][nt][2 * h + 1], sym);
+      }
+}
+
+// ---- TF32x3 trailing update with the split done once per CTA while staging ---------------
+// Chunk c + 1 of A (cold rows) and B (U rows) is loaded into registers while chunk c is
+// multiplied, then split into hi/lo TF32 words in the other stage: every operand value is
+// split once per tile instead of once per warp that reads it, and the inner loop is only
+// 32-bit shared loads and mma.sync.  Same split and product order as mma_chunk_tf32x3.
+struct SplitChunk {
+  double2 a[4], b[4];  // this thread's 8 of the chunk's 2 x 16 x 64 double2 pieces
+};
+
+__device__ __forceinline__ void load_split_chunk(SplitChunk& r, const double* A, long long lda, const double* B, long long ldb, int k_row0) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int piece = tid + i * kGemmThreads;
+    const long long off_a = (long long)(k_row0 + (piece >> 6)) * lda + (piece & 63) * 2;
+    const long long off_b = (long long)(k_row0 + (piece >> 6)) * ldb + (piece & 63) * 2;
+    r.a[i] = *reinterpret_cast<const double2*>(A + off_a);
+    r.b[i] = *reinterpret_cast<const double2*>(B + off_b);
+  }
+}
+
+__device__ __forceinline__ void store_split_chunk(const SplitChunk& r, unsigned* stage) {
+  const int tid = threadIdx.x;
+  unsigned* Ahi = stage;
+  unsigned* Alo = stage + kSplitArray;
+  unsigned* Bhi = stage + 2 * kSplitArray;
+  unsigned* Blo = stage + 3 * kSplitArray;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int piece = tid + i * kGemmThreads;
+    const int at = (piece >> 6) * kSplitLd + (piece & 63) * 2;
+    unsigned h0, l0, h1, l1;
+    split_tf32(r.a[i].x, h0, l0);
+    split_tf32(r.a[i].y, h1, l1);
+    *reinterpret_cast<uint2*>(Ahi + at) = make_uint2(h0, h1);
+    *reinterpret_cast<uint2*>(Alo + at) = make_uint2(l0, l1);
+    split_tf32(r.b[i].x, h0, l0);
+    split_tf32(r.b[i].y, h1, l1);
+    *reinterpret_cast<uint2*>(Bhi + at) = make_uint2(h0, h1);
+    *reinterpret_cast<uint2*>(Blo + at) = make_uint2(l0, l1);
+  }
+}
+
+__device__ __forceinline__ void mma_chunk_split(TileAcc32& acc, const unsigned* stage, int warp, int lane) {
+  const unsigned* Ahi = stage;
+  const unsigned* Alo = stage + kSplitArray;
+  const unsigned* Bhi = stage + 2 * kSplitArray;
+  const unsigned* Blo = stage + 3 * kSplitArray;
+  const int wm = (warp >> 2) * 64;
+  const int wn = (warp & 3) * 32;
+  const int t = lane & 3;
+  const int g = lane >> 2;
+#pragma unroll
+  for (int kk = 0; kk < kUpdChunk; kk += 8) {
+    unsigned ah[4][4], al[4][4], bh[4][2], bl[4][2];
+    const int r0 = (kk + t) * kSplitLd, r4 = (kk + t + 4) * kSplitLd;
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt) {
+      const int m = wm + mt * 16 + g;
+      ah[mt][0] = Ahi[r0 + m];
+      ah[mt][1] = Ahi[r0 + m + 8];
+      ah[mt][2] = Ahi[r4 + m];
+      ah[mt][3] = Ahi[r4 + m + 8];
+      al[mt][0] = Alo[r0 + m];
+      al[mt][1] = Alo[r0 + m + 8];
+      al[mt][2] = Alo[r4 + m];
+      al[mt][3] = Alo[r4 + m + 8];
+    }
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      const int n = wn + nt * 8 + g;
+      bh[nt][0] = Bhi[r0 + n];
+      bh[nt][1] = Bhi[r4 + n];
+      bl[nt][0] = Blo[r0 + n];
+      bl[nt][1] = Blo[r4 + n];
+    }
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        mma_tf32(acc.v[mt][nt], al[mt], bh[nt][0], bh[nt][1]);
+        mma_tf32(acc.v[mt][nt], ah[mt], bl[nt][0], bl[nt][1]);
+        mma_tf32(acc.v[mt][nt], ah[mt], bh[nt][0], bh[nt][1]);
+      }
+  }
+}
+
+// acc = A^T B over K = kBlock rows with chunk 0 already in `r`; on return `r` is free, the
+// stages are free (ends with a __syncthreads()) and the C tile's cp.async group is untouched.
+__device__ inline void split_mainloop(TileAcc32& acc, SplitChunk& r, const double* A, long long lda, const double* B, long long ldb, unsigned* stages) {
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  constexpr int nchunks = kBlock / kUpdChunk;
+  acc_zero(acc);
+  store_split_chunk(r, stages);
+  __syncthreads();
+#pragma unroll 1
+  for (int c = 0; c < nchunks; ++c) {
+    if (c + 1 < nchunks) load_split_chunk(r, A, lda, B, ldb, (c + 1) * kUpdChunk);
+    mma_chunk_split(acc, stages + (c & 1) * kSplitStageWords, warp, lane);
+    if (c + 1 < nchunks) store_split_chunk(r, stages + ((c + 1) & 1) * kSplitStageWords);
+    __syncthreads();
+  }
 }
 
 }  // namespace ticc

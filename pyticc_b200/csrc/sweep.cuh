@@ -477,10 +477,66 @@ __device__ inline void update_tiles(double* M, long long mstride, int ld, int kb
       update_tile_of<kSym>(gn, per, t, kb, bn, tan, tbn);
       issue_update_chunk0(cold + (long long)bn * cstride + tan * kBlock, ld, M + (long long)bn * mstride + (long long)k0 * ld + tbn * kBlock, ld, smem);
     }
-    // off-diagonal tiles of the symmetric sweep write their transpose from registers
-    acc_sub_smem(acc, Cs, Mb + (long long)c0 * ld + r0, ld, kSym && r0 != c0);
+    // C - acc straight from registers (with the transpose of an off-diagonal tile of the
+    // symmetric sweep, a diagonal tile symmetrised from its lower half); Cs is free after
+    acc_epilogue_direct(acc, Cs, Mb, ld, r0, c0, kSym);
     __syncthreads();
-    store_tile(Mb, ld, r0, c0, Cs, kSym && r0 == c0);  // a diagonal tile symmetrised from its lower half
+    if (gn >= total) break;
+    issue_update_ctile(Cs, M + (long long)bn * mstride + (long long)tan * kBlock * ld + tbn * kBlock, ld);
+    b = bn;
+    ta = tan;
+    tb = tbn;
+  }
+}
+
+// The same persistent tile loop for the TF32x3 steps, with the operands split while staging:
+// the next tile's first chunk goes into registers before the current tile's epilogue.
+template <bool kSym>
+__device__ inline void update_tiles_split(double* M, long long mstride, int ld, int kb, const double* cold, long long cstride, int t, int per, int total, bool skip_pivot,
+                                          int* queue, double* smem) {
+  const int tid = threadIdx.x;
+  double* Cs = smem + kUpdStageDoubles;
+  unsigned* stages = reinterpret_cast<unsigned*>(smem);
+  int* slot = reinterpret_cast<int*>(Cs + kBlock * kStride);
+  const int k0 = kb * kBlock;
+  auto fetch = [&]() {
+    if (tid == 0) {
+      int g = atomicAdd(queue, 1);
+      for (;;) {
+        if (g >= total || !skip_pivot) break;
+        int b, ta, tb;
+        update_tile_of<kSym>(g, per, t, kb, b, ta, tb);
+        if (ta != kb + 1 || tb != kb + 1) break;
+        g = atomicAdd(queue, 1);  // the pivot tile belongs to a pivot CTA
+      }
+      *slot = g;
+    }
+    __syncthreads();
+    const int g = *slot;
+    __syncthreads();
+    return g;
+  };
+  int g = fetch();
+  if (g >= total) return;
+  int b, ta, tb;
+  update_tile_of<kSym>(g, per, t, kb, b, ta, tb);
+  SplitChunk r;
+  load_split_chunk(r, cold + (long long)b * cstride + ta * kBlock, ld, M + (long long)b * mstride + (long long)k0 * ld + tb * kBlock, ld, 0);
+  issue_update_ctile(Cs, M + (long long)b * mstride + (long long)ta * kBlock * ld + tb * kBlock, ld);
+  for (;;) {
+    double* Mb = M + (long long)b * mstride;
+    const int r0 = ta * kBlock, c0 = tb * kBlock;
+    TileAcc32 acc;
+    split_mainloop(acc, r, cold + (long long)b * cstride + r0, ld, Mb + (long long)k0 * ld + c0, ld, stages);
+    const int gn = fetch();
+    int bn = 0, tan = 0, tbn = 0;
+    if (gn < total) {
+      update_tile_of<kSym>(gn, per, t, kb, bn, tan, tbn);
+      load_split_chunk(r, cold + (long long)bn * cstride + tan * kBlock, ld, M + (long long)bn * mstride + (long long)k0 * ld + tbn * kBlock, ld, 0);
+    }
+    cp_async_wait<0>();  // the C tile
+    __syncthreads();
+    acc_epilogue_direct(acc, Cs, Mb, ld, r0, c0, kSym);
     __syncthreads();
     if (gn >= total) break;
     issue_update_ctile(Cs, M + (long long)bn * mstride + (long long)tan * kBlock * ld + tbn * kBlock, ld);
@@ -535,7 +591,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) sweep_update_kernel(double* _
     __syncthreads();
   }
   if (reduced) {
-    update_tiles<kSym, TileAcc32>(M, mstride, ld, kb, cold, cstride, t, per, total, fuse_next != 0, queue, smem);
+    update_tiles_split<kSym>(M, mstride, ld, kb, cold, cstride, t, per, total, fuse_next != 0, queue, smem);
   } else {
     update_tiles<kSym, TileAcc>(M, mstride, ld, kb, cold, cstride, t, per, total, fuse_next != 0, queue, smem);
   }
