@@ -30,6 +30,7 @@ DEVICE_STATUS_TEXT = {
     3: "a Bessel continued fraction did not converge or produced a non-finite value",
     4: "asymptotic matching is undefined exactly at a channel threshold",
     5: "more open channels than the workspace was sized for",
+    6: "a fused sweep step gave up waiting for a row-panel tile (internal error; the wait is bounded)",
 }
 
 _P = ctypes.c_void_p

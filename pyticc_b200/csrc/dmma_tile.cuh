@@ -474,8 +474,8 @@ __device__ __forceinline__ void load_split_chunk(SplitChunk& r, const double* A,
     const int piece = tid + i * kGemmThreads;
     const long long off_a = (long long)(k_row0 + (piece >> 6)) * lda + (piece & 63) * 2;
     const long long off_b = (long long)(k_row0 + (piece >> 6)) * ldb + (piece & 63) * 2;
-    r.a[i] = *reinterpret_cast<const double2*>(A + off_a);
-    r.b[i] = *reinterpret_cast<const double2*>(B + off_b);
+    r.a[i] = __ldcg(reinterpret_cast<const double2*>(A + off_a));  // L2: written by other CTAs of a fused step
+    r.b[i] = __ldcg(reinterpret_cast<const double2*>(B + off_b));
   }
 }
 

@@ -182,99 +182,127 @@ __device__ __forceinline__ void put_padding(double* Mb, int np, long long r, lon
 // phase 1: A = [Q_end' + y1' + y2' S y2'] + Q_start + y1   (S from the previous sector)
 // phase 2: B = 2 Q_mid + 2 y1 + y2 S y2
 // phase 3: Y_out = Q_end + y1 + y2 S y2     (last sector of the call)
-// One CTA per (logical row i, batch item b = block * n_energy + energy): the row's
-// reference values are read once, the threads run along j (coalesced M, W and y2
-// accesses, no per-element index division).
+// One CTA per (logical row i, channel block g) runs over every energy of the block: the
+// row's W (or Q_mid) values are read once into registers and reused for all energies, and
+// each thread keeps kRowCols columns of loads in flight per energy.
+constexpr int kRowCols = 4;
 __global__ void __launch_bounds__(256) ldmd_elementwise_kernel(int phase, int s, LdmdSectors sec, LdmdLayout L, const double* Yin, double* Yout) {
   const int i = blockIdx.x;
-  const int e = blockIdx.y;  // batch item
-  const int g = e / L.n_energy;
-  const int batch = L.n_block * L.n_energy;
+  const int g = blockIdx.y;
+  const int ne = L.n_energy;
+  const int batch = L.n_block * ne;
   const int n = L.n, np = L.np;
   const int nl = L.is_complex ? np / 2 : np;  // logical-element grid covering the padded matrix
-  double* Mb = L.M + (long long)e * np * np;
   if (i >= n) {  // padding row
     if (phase == 3) return;
-    for (int j = threadIdx.x; j < nl; j += blockDim.x) {
-      if (L.is_complex) {
-        for (int a = 0; a < 2; ++a)
-          for (int b = 0; b < 2; ++b) put_padding(Mb, np, 2LL * i + a, 2LL * j + b);
-      } else {
-        put_padding(Mb, np, i, j);
+    for (int e = 0; e < ne; ++e) {
+      double* Mb = L.M + (long long)(g * ne + e) * np * np;
+      for (int j = threadIdx.x; j < nl; j += blockDim.x) {
+        if (L.is_complex) {
+          for (int a = 0; a < 2; ++a)
+            for (int c = 0; c < 2; ++c) put_padding(Mb, np, 2LL * i + a, 2LL * j + c);
+        } else {
+          put_padding(Mb, np, i, j);
+        }
       }
     }
     return;
   }
   const double h = sec.h[s];
   const long long wb = g * sec.wb_stride;
-  const double* y1 = L.y1 + ((long long)s * batch + e) * n;
-  const double* y2 = L.y2 + ((long long)s * batch + e) * n;
   const double* Ws = sec.Ws + s * sec.ws_stride + wb + (long long)i * n;
   const double* Wm = sec.Wm + s * sec.wm_stride + wb;
   const double* We = sec.We + s * sec.we_stride + wb + (long long)i * n;
   const double ref = Wm[(long long)i * n + i];
-  const double y1i = y1[i], y2i = y2[i];
-  // previous sector (phase 1)
-  double hp = 0.0, ref_p = 0.0, y1pi = 0.0, y2pi = 0.0;
+  double hp = 0.0, ref_p = 0.0;
   const double* Wep = nullptr;
-  const double* y2p = nullptr;
   if (phase == 1) {
     hp = sec.h[s - 1];
     Wep = sec.We + (s - 1) * sec.we_stride + wb + (long long)i * n;
-    const double* y1p = L.y1 + ((long long)(s - 1) * batch + e) * n;
-    y2p = L.y2 + ((long long)(s - 1) * batch + e) * n;
     ref_p = sec.Wm[(s - 1) * sec.wm_stride + wb + (long long)i * n + i];
-    y1pi = y1p[i];
-    y2pi = y2p[i];
   }
   const double* Qrow = L.Qm + ((long long)s * L.n_block + g) * L.npr * L.npr + (long long)i * L.npr;
-  for (int j = threadIdx.x; j < nl; j += blockDim.x) {
-    if (j >= n) {  // padding column
-      if (phase == 3) continue;
-      if (L.is_complex) {
-        for (int a = 0; a < 2; ++a)
-          for (int b = 0; b < 2; ++b) put_padding(Mb, np, 2LL * i + a, 2LL * j + b);
-      } else {
-        put_padding(Mb, np, i, j);
+  for (int j0 = 0; j0 < nl; j0 += kRowCols * 256) {
+    // energy-independent row values of this thread's columns
+    double wa[kRowCols], wp[kRowCols];
+#pragma unroll
+    for (int q = 0; q < kRowCols; ++q) {
+      const int j = j0 + q * 256 + threadIdx.x;
+      wa[q] = wp[q] = 0.0;
+      if (j < n) {
+        if (phase <= 1) wa[q] = Ws[j];
+        else if (phase == 2) wa[q] = Qrow[j];
+        else wa[q] = We[j];
+        if (phase == 1) wp[q] = Wep[j];
       }
-      continue;
     }
-    const double d = (i == j) ? 1.0 : 0.0;
-    double x = 0.0, z = 0.0;
-    if (phase == 0) {
-      if (L.is_complex) {
-        const double* Yb = Yin + (long long)e * n * n * 2;
-        x = 0.5 * (Yb[2 * ((long long)i * n + j)] + Yb[2 * ((long long)j * n + i)]);
-        z = 0.5 * (Yb[2 * ((long long)i * n + j) + 1] + Yb[2 * ((long long)j * n + i) + 1]);
-      } else {
-        const double* Yb = Yin + (long long)e * n * n;
-        x = 0.5 * (Yb[(long long)i * n + j] + Yb[(long long)j * n + i]);
+#pragma unroll 1
+    for (int e = 0; e < ne; ++e) {
+      const int b = g * ne + e;
+      double* Mb = L.M + (long long)b * np * np;
+      const double* y1 = L.y1 + ((long long)s * batch + b) * n;
+      const double* y2 = L.y2 + ((long long)s * batch + b) * n;
+      const double y1i = y1[i], y2i = y2[i];
+      double y1pi = 0.0, y2pi = 0.0;
+      const double* y2p = nullptr;
+      if (phase == 1) {
+        const double* y1p = L.y1 + ((long long)(s - 1) * batch + b) * n;
+        y2p = L.y2 + ((long long)(s - 1) * batch + b) * n;
+        y1pi = y1p[i];
+        y2pi = y2p[i];
       }
-    } else if (phase == 1) {
-      double sr, si;
-      get_swept(Mb, np, i, j, L.is_complex, sr, si);
-      x = hp * (Wep[j] - d * ref_p) / 3.0 + d * y1pi + y2pi * sr * y2p[j];
-      z = y2pi * si * y2p[j];
-    }
-    if (phase <= 1) {
-      x += h * (Ws[j] - d * ref) / 3.0 + d * y1i;
-      put_element(Mb, np, i, j, x, z, L.is_complex);
-    } else if (phase == 2) {
-      double sr, si;
-      get_swept(Mb, np, i, j, L.is_complex, sr, si);
-      x = 2.0 * Qrow[j] + 2.0 * d * y1i + y2i * sr * y2[j];
-      z = y2i * si * y2[j];
-      put_element(Mb, np, i, j, x, z, L.is_complex);
-    } else {
-      double sr, si;
-      get_swept(Mb, np, i, j, L.is_complex, sr, si);
-      x = h * (We[j] - d * ref) / 3.0 + d * y1i + y2i * sr * y2[j];
-      z = y2i * si * y2[j];
-      if (L.is_complex) {
-        Yout[((long long)e * n * n + (long long)i * n + j) * 2] = x;
-        Yout[((long long)e * n * n + (long long)i * n + j) * 2 + 1] = z;
-      } else {
-        Yout[(long long)e * n * n + (long long)i * n + j] = x;
+#pragma unroll
+      for (int q = 0; q < kRowCols; ++q) {
+        const int j = j0 + q * 256 + threadIdx.x;
+        if (j >= nl) continue;
+        if (j >= n) {  // padding column
+          if (phase == 3) continue;
+          if (L.is_complex) {
+            for (int a = 0; a < 2; ++a)
+              for (int c = 0; c < 2; ++c) put_padding(Mb, np, 2LL * i + a, 2LL * j + c);
+          } else {
+            put_padding(Mb, np, i, j);
+          }
+          continue;
+        }
+        const double d = (i == j) ? 1.0 : 0.0;
+        double x = 0.0, z = 0.0;
+        if (phase == 0) {
+          if (L.is_complex) {
+            const double* Yb = Yin + (long long)b * n * n * 2;
+            x = 0.5 * (Yb[2 * ((long long)i * n + j)] + Yb[2 * ((long long)j * n + i)]);
+            z = 0.5 * (Yb[2 * ((long long)i * n + j) + 1] + Yb[2 * ((long long)j * n + i) + 1]);
+          } else {
+            const double* Yb = Yin + (long long)b * n * n;
+            x = 0.5 * (Yb[(long long)i * n + j] + Yb[(long long)j * n + i]);
+          }
+        } else if (phase == 1) {
+          double sr, si;
+          get_swept(Mb, np, i, j, L.is_complex, sr, si);
+          x = hp * (wp[q] - d * ref_p) / 3.0 + d * y1pi + y2pi * sr * y2p[j];
+          z = y2pi * si * y2p[j];
+        }
+        if (phase <= 1) {
+          x += h * (wa[q] - d * ref) / 3.0 + d * y1i;
+          put_element(Mb, np, i, j, x, z, L.is_complex);
+        } else if (phase == 2) {
+          double sr, si;
+          get_swept(Mb, np, i, j, L.is_complex, sr, si);
+          x = 2.0 * wa[q] + 2.0 * d * y1i + y2i * sr * y2[j];
+          z = y2i * si * y2[j];
+          put_element(Mb, np, i, j, x, z, L.is_complex);
+        } else {
+          double sr, si;
+          get_swept(Mb, np, i, j, L.is_complex, sr, si);
+          x = h * (wa[q] - d * ref) / 3.0 + d * y1i + y2i * sr * y2[j];
+          z = y2i * si * y2[j];
+          if (L.is_complex) {
+            Yout[((long long)b * n * n + (long long)i * n + j) * 2] = x;
+            Yout[((long long)b * n * n + (long long)i * n + j) * 2 + 1] = z;
+          } else {
+            Yout[(long long)b * n * n + (long long)i * n + j] = x;
+          }
+        }
       }
     }
   }
@@ -317,7 +345,7 @@ inline cudaError_t ldmd_propagate(double* Y, const double* energies, double mu, 
   cudaError_t err = ldmd_qmid(sec, L, status, stream);
   if (err != cudaSuccess) return err;
   const long long nl = L.is_complex ? L.np / 2 : L.np;
-  const dim3 grid((unsigned)nl, batch);
+  const dim3 grid((unsigned)nl, L.n_block);
   const long long mstride = (long long)L.np * L.np;
   const int used = L.is_complex ? 2 * L.n : L.n;  // rows of the work matrix beyond these are identity padding
   for (int s = 0; s < sec.n_sector; ++s) {

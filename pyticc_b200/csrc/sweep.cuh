@@ -316,7 +316,7 @@ __device__ inline void copy_tile(double* dst, int ldd, int dr0, int dc0, const d
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int piece = base + u * kGemmThreads + tid;
-      m[u] = *reinterpret_cast<const double2*>(src + (long long)(sr0 + (piece >> 6)) * lds + sc0 + (piece & 63) * 2);
+      m[u] = __ldcg(reinterpret_cast<const double2*>(src + (long long)(sr0 + (piece >> 6)) * lds + sc0 + (piece & 63) * 2));
     }
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
@@ -597,6 +597,161 @@ __global__ void __launch_bounds__(kGemmThreads, 1) sweep_update_kernel(double* _
   }
 }
 
+// ---- one persistent launch per step of the symmetric sweep ---------------------------------
+// Work units from one queue, in order: the step's row-panel tiles (matrix b, column tile jt),
+// then the fused next-pivot units (one per matrix), then the trailing-update tiles.  A unit
+// waits only for row-panel tiles, which come earlier in the queue and so were fetched by
+// CTAs that are already running: the waits cannot deadlock.  Each wait is still bounded; on
+// timeout the CTA raises a shared abort flag, reports kDeviceStalled and skips the unit.
+// Flags hold the step number + 1 of the last finished row-panel tile; queues alternate by
+// step parity (each step resets the next step's) and so do the two P^-1 slots of a matrix
+// (a pivot unit writes the next step's slot while row-panel tiles still read this one).
+// Per-matrix integer area (the 16-double tail of the sweep scratch): [0..1] queues (matrix 0),
+// [2] abort flag (matrix 0), [4 .. 4 + nt) row-panel flags.
+constexpr int kStepFlagOffset = 4;
+constexpr int kStepIntsPerMatrix = 32;
+constexpr long long kStepSpinLimit = 1LL << 22;
+
+__device__ __forceinline__ int load_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void store_release(int* p, int v) { asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory"); }
+
+// Thread 0 waits until both flags reach `target`; the CTA learns the outcome.
+__device__ inline bool step_wait(const int* f0, const int* f1, int target, int* abort_flag, int* status, int b, int* slot) {
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    for (long long it = 0;; ++it) {
+      if (load_acquire(f0) >= target && load_acquire(f1) >= target) break;
+      if (load_acquire(abort_flag) != 0 || it >= kStepSpinLimit) {
+        if (atomicExch(abort_flag, 1) == 0) report_status(status, kDeviceStalled, b, target);
+        ok = 0;
+        break;
+      }
+      __nanosleep(128);
+    }
+    *slot = ok;
+  }
+  __syncthreads();
+  const bool ok = *slot != 0;
+  __syncthreads();
+  return ok;
+}
+
+// Row-panel tile (b, jt) of step kb: keep the old rows K in `cold`, U = P^-1 M_KR, U into
+// the rows K and U^T into the columns K.  Pt is this matrix's P^-1 for the step.
+__device__ inline void rowpanel_unit(double* Mb, int ld, int kb, int jt, const double* Pt, double* Cb, double* smem) {
+  const int k0 = kb * kBlock, c0 = jt * kBlock;
+  copy_tile(Cb, ld, 0, c0, Mb, ld, k0, c0);
+  TileAcc acc;
+  tile_gemm_tn(acc, Pt, kBlock, Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
+  acc_to_smem_mirror(acc, smem, Mb + (long long)c0 * ld + k0, ld, true);
+  __syncthreads();
+  store_tile(Mb, ld, k0, c0, smem, false);
+}
+
+template <class Acc>
+__device__ inline void update_unit(Acc& acc, double* Mb, int ld, int k0, int r0, int c0, const double* Cb, double* smem) {
+  double* Cs = smem + kUpdStageDoubles;
+  tile_update_product(acc, Cb + r0, ld, Mb + (long long)k0 * ld + c0, ld, kBlock, smem, Cs, Mb + (long long)r0 * ld + c0, ld);
+  acc_epilogue_direct(acc, Cs, Mb, ld, r0, c0, true);
+  __syncthreads();
+}
+
+__device__ inline void update_unit_split(double* Mb, int ld, int k0, int r0, int c0, const double* Cb, double* smem) {
+  double* Cs = smem + kUpdStageDoubles;
+  SplitChunk r;
+  load_split_chunk(r, Cb + r0, ld, Mb + (long long)k0 * ld + c0, ld, 0);
+  issue_update_ctile(Cs, Mb + (long long)r0 * ld + c0, ld);
+  TileAcc32 acc;
+  split_mainloop(acc, r, Cb + r0, ld, Mb + (long long)k0 * ld + c0, ld, reinterpret_cast<unsigned*>(smem));
+  cp_async_wait<0>();
+  __syncthreads();
+  acc_epilogue_direct(acc, Cs, Mb, ld, r0, c0, true);
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kGemmThreads, 1) sweep_step_kernel(double* __restrict__ M, long long mstride, int ld, int kb, double* __restrict__ cold, long long cstride, int t, int batch, int fuse_next, double* __restrict__ pinv, int* status, const int* __restrict__ reduced_blocks, int* ints) {
+  extern __shared__ double smem[];
+  const int tid = threadIdx.x;
+  int* slot = reinterpret_cast<int*>(smem + kUpdStageDoubles + kBlock * kStride);
+  int* queue = ints + (kb & 1);
+  int* abort_flag = ints + 2;
+  if (blockIdx.x == 0 && tid == 0) ints[(kb + 1) & 1] = 0;  // the next step's queue
+  const int per = t * (t + 1) / 2;
+  const int n_panel = t * batch;
+  const int n_pivot = fuse_next ? batch : 0;
+  const int total = n_panel + n_pivot + per * batch;
+  const int k0 = kb * kBlock;
+  const int pslot = kb & 1, nslot = (kb + 1) & 1;
+  const bool reduced = reduced_blocks != nullptr && kb < *reduced_blocks;
+  for (;;) {
+    if (tid == 0) *slot = atomicAdd(queue, 1);
+    __syncthreads();
+    const int u = *slot;
+    __syncthreads();
+    if (u >= total) break;
+    if (u < n_panel) {
+      const int b = u / t, j = u % t;
+      const int jt = j + (j >= kb ? 1 : 0);
+      double* Mb = M + (long long)b * mstride;
+      rowpanel_unit(Mb, ld, kb, jt, pinv + (long long)b * 2 * kBlock * kBlock + pslot * kBlock * kBlock, cold + (long long)b * cstride, smem);
+      __syncthreads();
+      if (tid == 0) {
+        __threadfence();
+        store_release(ints + b * kStepIntsPerMatrix + kStepFlagOffset + jt, kb + 1);
+      }
+      continue;
+    }
+    if (u < n_panel + n_pivot) {
+      const int b = u - n_panel;
+      const int p0 = (kb + 1) * kBlock;
+      const int* f = ints + b * kStepIntsPerMatrix + kStepFlagOffset + kb + 1;
+      if (!step_wait(f, f, kb + 1, abort_flag, status, b, slot)) continue;
+      double* Mb = M + (long long)b * mstride;
+      double* Cs = smem + kUpdStageDoubles;
+      const double* A = cold + (long long)b * cstride + p0;
+      const double* B = Mb + (long long)k0 * ld + p0;
+      const double* Cg = Mb + (long long)p0 * ld + p0;
+      if (reduced) {
+        TileAcc32 acc;
+        tile_update_product(acc, A, ld, B, ld, kBlock, smem, Cs, Cg, ld);
+        acc_sub_smem(acc, Cs, Mb, ld, false);
+      } else {
+        TileAcc acc;
+        tile_update_product(acc, A, ld, B, ld, kBlock, smem, Cs, Cg, ld);
+        acc_sub_smem(acc, Cs, Mb, ld, false);
+      }
+      __syncthreads();
+      for (int e = tid; e < kBlock * kBlock; e += kGemmThreads) {  // symmetrise from the lower half
+        const int r = e >> 7, c = e & (kBlock - 1);
+        if (r < c) Cs[r * kStride + c] = Cs[c * kStride + r];
+      }
+      __syncthreads();
+      invert_pivot_block<true>(Cs, smem, Mb, ld, p0, pinv + nslot * kBlock * kBlock, b, status);
+      __syncthreads();
+      continue;
+    }
+    const int g = u - n_panel - n_pivot;
+    int b, ta, tb;
+    update_tile_of<true>(g, per, t, kb, b, ta, tb);
+    if (fuse_next && ta == kb + 1 && tb == kb + 1) continue;  // the pivot unit's tile
+    const int* fa = ints + b * kStepIntsPerMatrix + kStepFlagOffset + ta;
+    const int* fb = ints + b * kStepIntsPerMatrix + kStepFlagOffset + tb;
+    if (!step_wait(fa, fb, kb + 1, abort_flag, status, b, slot)) continue;
+    double* Mb = M + (long long)b * mstride;
+    const double* Cb = cold + (long long)b * cstride;
+    if (reduced) {
+      update_unit_split(Mb, ld, k0, ta * kBlock, tb * kBlock, Cb, smem);
+    } else {
+      TileAcc acc;
+      update_unit(acc, Mb, ld, k0, ta * kBlock, tb * kBlock, Cb, smem);
+    }
+  }
+}
+
 // Scratch per matrix: cold (kBlock x np) + P^-1 and its transpose (2 x kBlock x kBlock).
 // The last 16 doubles of each matrix's share hold the update kernel's tile queue (one int).
 inline size_t sweep_scratch_doubles(int np) { return size_t(kBlock) * np + size_t(2) * kBlock * kBlock + 16; }
@@ -612,11 +767,15 @@ inline cudaError_t sweep_configure_variant() {
   return cudaFuncSetAttribute(sweep_update_kernel<kSym>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmemBytes);
 }
 
+inline cudaError_t sweep_configure_step() { return cudaFuncSetAttribute(sweep_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmemBytes); }
+
 inline cudaError_t sweep_configure() {
   // per-device attribute: cheap to repeat, so no process-wide cache is kept
   cudaError_t e = sweep_configure_variant<true>();
   if (e != cudaSuccess) return e;
   e = sweep_configure_variant<false>();
+  if (e != cudaSuccess) return e;
+  e = sweep_configure_step();
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(sweep_colpanel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmemBytes);
 }
@@ -646,8 +805,25 @@ inline cudaError_t sweep_batched(double* M, long long mstride, int np, int batch
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
   }
+  const bool fused = kSym && nt >= 2 && nt <= kStepIntsPerMatrix - kStepFlagOffset;
+  if (fused) {
+    e = cudaMemsetAsync(queue, 0, sizeof(int) * kStepIntsPerMatrix * (size_t)batch, stream);
+    if (e != cudaSuccess) return e;
+  }
   sweep_pivot_kernel<kSym><<<batch, kPivotThreads, kPivotSmemBytes, stream>>>(M, mstride, np, 0, pinv, status);
   note_launch();
+  if (fused) {
+    const int t = nt - 1;
+    const long long per = (long long)t * (t + 1) / 2;
+    for (int kb = 0; kb < nt; ++kb) {
+      const int fuse = (kb + 1 < nt) ? 1 : 0;
+      const long long work = (long long)t * batch + (fuse ? batch : 0) + per * batch;
+      const long long blocks = work < sms ? work : sms;
+      sweep_step_kernel<<<(unsigned)blocks, kGemmThreads, kUpdateSmemBytes, stream>>>(M, mstride, np, kb, cold, cstride, t, batch, fuse, pinv, status, reduced_blocks, queue);
+      note_launch();
+    }
+    return cudaGetLastError();
+  }
   for (int kb = 0; kb < nt; ++kb) {
     if (nt == 1) break;
     const int t = nt - 1;

@@ -34,6 +34,7 @@ enum DeviceStatus : int {
   kDeviceNonFinite = 2,       // a non-finite value reached an output
   kDeviceBesselFailed = 3,    // a Bessel continued fraction did not converge
   kDeviceThreshold = 4,       // a total energy sits exactly on a channel threshold
+  kDeviceStalled = 6,         // a fused sweep step gave up waiting for a row-panel tile (bounded wait)
 };
 
 // Host-side count of kernels this library has enqueued (process lifetime).
