@@ -235,6 +235,32 @@ __device__ inline void tile_gemm_tn_tf32x3(TileAcc32& acc, const double* A, long
   }
 }
 
+// acc32 into a [128][kStride] shared tile and, with `mirror`, its transpose to Mt (row
+// stride ld) straight from registers, as acc_to_smem_mirror.
+__device__ __forceinline__ void acc32_to_smem_mirror(const TileAcc32& acc, double* Cs, double* Mt, long long ld, bool mirror) {
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  const int wm = (warp >> 2) * 64;
+  const int wn = (warp & 3) * 32;
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int row = wm + mt * 16 + g + 8 * h, col = wn + nt * 8 + 2 * t;
+        const double v0 = acc.v[mt][nt][2 * h], v1 = acc.v[mt][nt][2 * h + 1];
+        Cs[row * kStride + col] = v0;
+        Cs[row * kStride + col + 1] = v1;
+        if (mirror) {
+          Mt[(long long)col * ld + row] = v0;
+          Mt[(long long)(col + 1) * ld + row] = v1;
+        }
+      }
+}
+
 __device__ __forceinline__ void acc32_to_smem(const TileAcc32& acc, double* Cs, double scale) {
   const int tid = threadIdx.x;
   const int warp = tid >> 5;

@@ -641,13 +641,21 @@ __device__ inline bool step_wait(const int* f0, const int* f1, int target, int* 
 }
 
 // Row-panel tile (b, jt) of step kb: keep the old rows K in `cold`, U = P^-1 M_KR, U into
-// the rows K and U^T into the columns K.  Pt is this matrix's P^-1 for the step.
-__device__ inline void rowpanel_unit(double* Mb, int ld, int kb, int jt, const double* Pt, double* Cb, double* smem) {
+// the rows K and U^T into the columns K.  Pt is this matrix's P^-1 for the step.  When the
+// pivot block K is strongly closed (`reduced`), U takes the same FP32-accurate TF32x3
+// product as the step's trailing update.
+__device__ inline void rowpanel_unit(double* Mb, int ld, int kb, int jt, const double* Pt, double* Cb, double* smem, bool reduced) {
   const int k0 = kb * kBlock, c0 = jt * kBlock;
   copy_tile(Cb, ld, 0, c0, Mb, ld, k0, c0);
-  TileAcc acc;
-  tile_gemm_tn(acc, Pt, kBlock, Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
-  acc_to_smem_mirror(acc, smem, Mb + (long long)c0 * ld + k0, ld, true);
+  if (reduced) {
+    TileAcc32 acc;
+    tile_gemm_tn_tf32x3(acc, Pt, kBlock, Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
+    acc32_to_smem_mirror(acc, smem, Mb + (long long)c0 * ld + k0, ld, true);
+  } else {
+    TileAcc acc;
+    tile_gemm_tn(acc, Pt, kBlock, Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
+    acc_to_smem_mirror(acc, smem, Mb + (long long)c0 * ld + k0, ld, true);
+  }
   __syncthreads();
   store_tile(Mb, ld, k0, c0, smem, false);
 }
@@ -697,7 +705,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) sweep_step_kernel(double* __r
       const int b = u / t, j = u % t;
       const int jt = j + (j >= kb ? 1 : 0);
       double* Mb = M + (long long)b * mstride;
-      rowpanel_unit(Mb, ld, kb, jt, pinv + (long long)b * 2 * kBlock * kBlock + pslot * kBlock * kBlock, cold + (long long)b * cstride, smem);
+      rowpanel_unit(Mb, ld, kb, jt, pinv + (long long)b * 2 * kBlock * kBlock + pslot * kBlock * kBlock, cold + (long long)b * cstride, smem, reduced);
       __syncthreads();
       if (tid == 0) {
         __threadfence();
