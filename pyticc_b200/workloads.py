@@ -138,3 +138,45 @@ def ultracold_capture(*, B_cm=0.03, jmax=40, J=10, parity=1, mu_amu=100.0, C6=1.
     energies = np.geomspace(1.0e-6, 1.0e-3, n_energy) * K2AU if energies_K is None else np.asarray(energies_K) * K2AU
     system = build_ScattSystem(AtomSpec(), rigid_rotor(B_cm, jmax), Jtot=J, system_parity=parity, potential=capture_pes(C6, wall_cm, seed), reduced_mass=mu_amu * AMU2AU, approx=approx, K_delta=K_delta)
     return Workload("ultracold_capture", system, prepare_potential(system, boundaries, half_steps, n_theta=n_theta), energies, mode="capture")
+
+
+def _propagate_window(argv=None) -> None:
+    """Propagate a window of the bench system's sectors once (a small, fixed case for
+    profilers): ``python -m pyticc_b200.workloads --precision mixed --first 100 --sectors 8``."""
+    import argparse
+
+    import torch
+
+    from .propagation.config import Propagation
+    from .propagation.runner import propagate
+    from .scattering import hamiltonian_for
+
+    p = argparse.ArgumentParser(description=_propagate_window.__doc__)
+    p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    p.add_argument("--first", type=int, default=100, help="first sector")
+    p.add_argument("--sectors", type=int, default=8)
+    p.add_argument("--energies", type=int, default=16, help="every 256/energies-th of the bench energies")
+    p.add_argument("--repeat", type=int, default=0, help="also time the LDMD launches this many times (CUDA events) and print the best ms per sector")
+    args = p.parse_args(argv)
+    wl = morse_atom_diatom()
+    ham = hamiltonian_for(wl.system, wl.grid)
+    energies = wl.energies[:: max(1, wl.energies.size // args.energies)][: args.energies]
+    sectors = wl.grid.sectors[args.first : args.first + args.sectors]
+    config = Propagation(precision=args.precision)
+    propagate(ham, energies, sectors, config)
+    torch.cuda.synchronize()
+    best = None
+    for _ in range(args.repeat):
+        windows: list = []
+        propagate(ham, energies, sectors, config, window_timing=windows)
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b, _ in windows)
+        best = ms if best is None else min(best, ms)
+    if best is not None:
+        flops = 2.0 * wl.system.basis.n_channel**3 * energies.size * len(sectors)
+        print(f"{args.precision}: {best / len(sectors):.2f} ms/sector (best of {args.repeat} x {len(sectors)} sectors), {flops / (best * 1e-3) / 1e12:.1f} TF/s")
+    print("ok")
+
+
+if __name__ == "__main__":
+    _propagate_window()
