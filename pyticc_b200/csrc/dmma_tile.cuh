@@ -428,17 +428,13 @@ __device__ __forceinline__ void acc_sub_smem(const TileAcc32& acc, double* Cs, d
 }
 
 // Epilogue written straight from the accumulator registers: M[r0 + row][c0 + col] = C - acc
-// with C from the staged tile Cs (a double2 per lane pair of columns).  An off-diagonal tile
-// of the symmetric sweep also writes its transpose (the 8 lanes sharing a column write 64
-// contiguous bytes); a diagonal tile writes each lower-half value (row >= col) to both of
-// its positions, so the tile stays exactly symmetric.  Cs is only read.
+// with C from the staged tile Cs (a double2 per lane pair of columns).  The symmetric sweep
+// keeps only the lower and diagonal 128-tiles current, so an off-diagonal tile writes no
+// transpose; a diagonal tile writes each lower-half value (row >= col) to both of its
+// positions, so the tile stays exactly symmetric.  Cs is only read.
 __device__ __forceinline__ void put_updated(double* Mb, long long ld, int r0, int c0, int row, int col, double v0, double v1, bool sym) {
   if (!sym || r0 != c0) {
     *reinterpret_cast<double2*>(Mb + (long long)(r0 + row) * ld + c0 + col) = make_double2(v0, v1);
-    if (sym) {
-      Mb[(long long)(c0 + col) * ld + r0 + row] = v0;
-      Mb[(long long)(c0 + col + 1) * ld + r0 + row] = v1;
-    }
   } else {
     if (row >= col) {
       Mb[(long long)(r0 + row) * ld + c0 + col] = v0;

@@ -162,8 +162,15 @@ __device__ __forceinline__ void put_element(double* Mb, int np, int i, int j, do
 }
 
 // Read the swept value S = -A^{-1} at logical (i, j): real part S00 and the imaginary
-// companion -S01 (so that -A^{-1} = s_re + i s_im).
+// companion -S01 (so that -A^{-1} = s_re + i s_im).  The symmetric sweep keeps only the
+// lower and diagonal 128-tiles current, so an element of an upper tile is read at (j, i).
 __device__ __forceinline__ void get_swept(const double* Mb, int np, int i, int j, int is_complex, double& s_re, double& s_im) {
+  const int mi = is_complex ? 2 * i : i, mj = is_complex ? 2 * j : j;
+  if ((mi >> 7) < (mj >> 7)) {
+    const int x = i;
+    i = j;
+    j = x;
+  }
   if (is_complex) {
     s_re = Mb[(long long)(2 * i) * np + 2 * j];
     s_im = -Mb[(long long)(2 * i) * np + 2 * j + 1];
@@ -184,7 +191,10 @@ __device__ __forceinline__ void put_padding(double* Mb, int np, long long r, lon
 // phase 3: Y_out = Q_end + y1 + y2 S y2     (last sector of the call)
 // One CTA per (logical row i, channel block g) runs over every energy of the block: the
 // row's W (or Q_mid) values are read once into registers and reused for all energies, and
-// each thread keeps kRowCols columns of loads in flight per energy.
+// each thread keeps kRowCols columns of loads in flight per energy.  Every quantity is
+// symmetric in (i, j) and the sweep reads only the lower and diagonal 128-tiles, so a row
+// is processed up to the end of its diagonal tile; the last pass writes Y_out's upper
+// triangle as the transpose of the lower tiles.
 constexpr int kRowCols = 4;
 __global__ void __launch_bounds__(256) ldmd_elementwise_kernel(int phase, int s, LdmdSectors sec, LdmdLayout L, const double* Yin, double* Yout) {
   const int i = blockIdx.x;
@@ -193,11 +203,15 @@ __global__ void __launch_bounds__(256) ldmd_elementwise_kernel(int phase, int s,
   const int batch = L.n_block * ne;
   const int n = L.n, np = L.np;
   const int nl = L.is_complex ? np / 2 : np;  // logical-element grid covering the padded matrix
+  const int mi = L.is_complex ? 2 * i : i;    // work-matrix row of logical row i
+  const int tile_end = ((mi >> 7) + 1) << 7;  // end of row i's diagonal 128-tile (work-matrix columns)
+  const int jl = L.is_complex ? tile_end / 2 : tile_end;
+  const int jlim = jl < nl ? jl : nl;
   if (i >= n) {  // padding row
     if (phase == 3) return;
     for (int e = 0; e < ne; ++e) {
       double* Mb = L.M + (long long)(g * ne + e) * np * np;
-      for (int j = threadIdx.x; j < nl; j += blockDim.x) {
+      for (int j = threadIdx.x; j < jlim; j += blockDim.x) {
         if (L.is_complex) {
           for (int a = 0; a < 2; ++a)
             for (int c = 0; c < 2; ++c) put_padding(Mb, np, 2LL * i + a, 2LL * j + c);
@@ -222,7 +236,7 @@ __global__ void __launch_bounds__(256) ldmd_elementwise_kernel(int phase, int s,
     ref_p = sec.Wm[(s - 1) * sec.wm_stride + wb + (long long)i * n + i];
   }
   const double* Qrow = L.Qm + ((long long)s * L.n_block + g) * L.npr * L.npr + (long long)i * L.npr;
-  for (int j0 = 0; j0 < nl; j0 += kRowCols * 256) {
+  for (int j0 = 0; j0 < jlim; j0 += kRowCols * 256) {
     // energy-independent row values of this thread's columns
     double wa[kRowCols], wp[kRowCols];
 #pragma unroll
@@ -254,7 +268,7 @@ __global__ void __launch_bounds__(256) ldmd_elementwise_kernel(int phase, int s,
 #pragma unroll
       for (int q = 0; q < kRowCols; ++q) {
         const int j = j0 + q * 256 + threadIdx.x;
-        if (j >= nl) continue;
+        if (j >= jlim) continue;
         if (j >= n) {  // padding column
           if (phase == 3) continue;
           if (L.is_complex) {
@@ -296,11 +310,17 @@ __global__ void __launch_bounds__(256) ldmd_elementwise_kernel(int phase, int s,
           get_swept(Mb, np, i, j, L.is_complex, sr, si);
           x = h * (wa[q] - d * ref) / 3.0 + d * y1i + y2i * sr * y2[j];
           z = y2i * si * y2[j];
+          const bool below = ((L.is_complex ? 2 * j : j) >> 7) < (mi >> 7);  // (i, j) in a strictly lower tile
           if (L.is_complex) {
             Yout[((long long)b * n * n + (long long)i * n + j) * 2] = x;
             Yout[((long long)b * n * n + (long long)i * n + j) * 2 + 1] = z;
+            if (below) {
+              Yout[((long long)b * n * n + (long long)j * n + i) * 2] = x;
+              Yout[((long long)b * n * n + (long long)j * n + i) * 2 + 1] = z;
+            }
           } else {
             Yout[(long long)b * n * n + (long long)i * n + j] = x;
+            if (below) Yout[(long long)b * n * n + (long long)j * n + i] = x;
           }
         }
       }

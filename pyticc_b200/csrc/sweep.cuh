@@ -326,6 +326,50 @@ __device__ inline void copy_tile(double* dst, int ldd, int dr0, int dc0, const d
   }
 }
 
+// dst[k][dc0 + c] = src[sr0 + c][sc0 + k] for a 128x128 tile, through a shared tile of row
+// stride 129 (conflict-free column reads; one double per thread and step, so the global
+// writes of a warp are 256 contiguous bytes).  Ends with a __syncthreads().
+constexpr int kTransLd = kBlock + 1;
+__device__ inline void copy_tile_transposed(double* dst, int ldd, int dc0, const double* src, int lds, int sr0, int sc0, double* smem) {
+  const int tid = threadIdx.x;
+#pragma unroll 1
+  for (int base = 0; base < kBlock * 64; base += 8 * kGemmThreads) {
+    double2 m[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int piece = base + u * kGemmThreads + tid;
+      m[u] = __ldcg(reinterpret_cast<const double2*>(src + (long long)(sr0 + (piece >> 6)) * lds + sc0 + (piece & 63) * 2));
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int piece = base + u * kGemmThreads + tid;
+      double* d = smem + (piece >> 6) * kTransLd + (piece & 63) * 2;
+      d[0] = m[u].x;
+      d[1] = m[u].y;
+    }
+  }
+  __syncthreads();
+#pragma unroll 4
+  for (int e = tid; e < kBlock * kBlock; e += kGemmThreads) {
+    const int k = e >> 7, c = e & (kBlock - 1);
+    dst[(long long)k * ldd + dc0 + c] = smem[c * kTransLd + k];
+  }
+  __syncthreads();
+}
+
+// The old rows K over column tile jt (M_KR, the tile that U = P^-1 M_KR needs) into cold.
+// Only the lower and diagonal 128-tiles of a symmetric work matrix are current, so for
+// jt > kb the tile is read as the transpose of (jt, kb).  Ends with a __syncthreads().
+__device__ inline void load_cold_tile(double* Cb, int ld, const double* Mb, int kb, int jt, double* smem) {
+  const int k0 = kb * kBlock, c0 = jt * kBlock;
+  if (jt < kb) {
+    copy_tile(Cb, ld, 0, c0, Mb, ld, k0, c0);
+    __syncthreads();
+  } else {
+    copy_tile_transposed(Cb, ld, c0, Mb, ld, c0, k0, smem);
+  }
+}
+
 // Write a finished 128x128 tile from shared memory to M at (r0, c0).  With `mirror`
 // (symmetric sweep) its transpose also goes to (c0, r0) and a diagonal tile is written
 // symmetrised from its lower half.
@@ -369,12 +413,14 @@ __global__ void __launch_bounds__(kGemmThreads) sweep_rowpanel_kernel(double* __
   double* Mb = M + (long long)b * mstride;
   double* Cb = cold + (long long)b * cstride;
   const int tid = threadIdx.x;
-  if (kSym) copy_tile(Cb, ld, 0, c0, Mb, ld, k0, c0);
+  if (kSym) load_cold_tile(Cb, ld, Mb, kb, jt, smem);
   const double* Pt = pinv + (long long)b * 2 * kBlock * kBlock + (kSym ? 0 : kBlock * kBlock);
   TileAcc acc;
-  tile_gemm_tn(acc, Pt, kBlock, Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
-  // U^T into the columns K from registers (symmetric sweep), U rows from shared memory
-  acc_to_smem_mirror(acc, smem, Mb + (long long)c0 * ld + k0, ld, kSym);
+  // the symmetric sweep reads M_KR from cold (current for every jt), the general one from M
+  tile_gemm_tn(acc, Pt, kBlock, kSym ? Cb + c0 : Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
+  // U^T into the columns K from registers where (jt, kb) is a lower tile, U rows (for jt > kb
+  // the otherwise unused upper tile, read by this step's update) from shared memory
+  acc_to_smem_mirror(acc, smem, Mb + (long long)c0 * ld + k0, ld, kSym && jt > kb);
   __syncthreads();
   store_tile(Mb, ld, k0, c0, smem, false);
   if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) *queue = 0;  // the step's update tile queue
@@ -641,20 +687,21 @@ __device__ inline bool step_wait(const int* f0, const int* f1, int target, int* 
 }
 
 // Row-panel tile (b, jt) of step kb: keep the old rows K in `cold`, U = P^-1 M_KR, U into
-// the rows K and U^T into the columns K.  Pt is this matrix's P^-1 for the step.  When the
+// the rows K and, where (jt, kb) is a lower tile, U^T into the columns K.  Pt is this
+// matrix's P^-1 for the step.  When the
 // pivot block K is strongly closed (`reduced`), U takes the same FP32-accurate TF32x3
 // product as the step's trailing update.
 __device__ inline void rowpanel_unit(double* Mb, int ld, int kb, int jt, const double* Pt, double* Cb, double* smem, bool reduced) {
   const int k0 = kb * kBlock, c0 = jt * kBlock;
-  copy_tile(Cb, ld, 0, c0, Mb, ld, k0, c0);
+  load_cold_tile(Cb, ld, Mb, kb, jt, smem);
   if (reduced) {
     TileAcc32 acc;
-    tile_gemm_tn_tf32x3(acc, Pt, kBlock, Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
-    acc32_to_smem_mirror(acc, smem, Mb + (long long)c0 * ld + k0, ld, true);
+    tile_gemm_tn_tf32x3(acc, Pt, kBlock, Cb + c0, ld, kBlock, smem);
+    acc32_to_smem_mirror(acc, smem, Mb + (long long)c0 * ld + k0, ld, jt > kb);
   } else {
     TileAcc acc;
-    tile_gemm_tn(acc, Pt, kBlock, Mb + (long long)k0 * ld + c0, ld, kBlock, smem);
-    acc_to_smem_mirror(acc, smem, Mb + (long long)c0 * ld + k0, ld, true);
+    tile_gemm_tn(acc, Pt, kBlock, Cb + c0, ld, kBlock, smem);
+    acc_to_smem_mirror(acc, smem, Mb + (long long)c0 * ld + k0, ld, jt > kb);
   }
   __syncthreads();
   store_tile(Mb, ld, k0, c0, smem, false);

@@ -56,6 +56,19 @@ def test_symmetric_sweep_inverse_real(n):
     np.testing.assert_array_equal(X, X.transpose(0, 2, 1))
 
 
+@pytest.mark.parametrize("n", [3584, 3713])
+def test_symmetric_sweep_inverse_at_the_fused_step_limit(n):
+    """28 pivot blocks (the largest sweep run as one persistent launch per step) and 30
+    (separate row-panel and update kernels); both keep only the lower tiles current."""
+    rng = np.random.default_rng(n)
+    A = rng.normal(size=(1, n, n))
+    A = A + A.transpose(0, 2, 1) + np.diag(rng.uniform(3.0, 6.0, n)) * np.sqrt(n) * np.sign(rng.normal(size=n))
+    X = _sym_inverse(A, False)
+    inv = np.linalg.inv(A)
+    np.testing.assert_allclose(X, inv, rtol=0, atol=1e-12 * np.abs(inv).max())
+    np.testing.assert_array_equal(X, X.transpose(0, 2, 1))
+
+
 @pytest.mark.parametrize("n", [300, 520])
 def test_symmetric_sweep_inverse_indefinite(n):
     """Random indefinite matrices: pivoting is local to each 128-wide block, so the error
