@@ -4,17 +4,22 @@
 // The sweep (principal pivot transform) over an index block K with P = M_KK:
 //     M_KK <- -P^{-1},   M_KR <- P^{-1} M_KR,   M_RK <- M_RK P^{-1},
 //     M_RR <- M_RR - M_RK P^{-1} M_KR,
-// keeps M symmetric, and sweeping every block in turn yields -M^{-1}.  Per block:
-//   1. pivot kernel   : one CTA per matrix inverts the 128x128 block P in shared
-//                       memory by Gauss-Jordan exchange with partial pivoting
-//                       (pivoting is local to the block), writes -P^{-1} into M_KK
-//                       and P^{-1} into a scratch buffer;
-//   2. row-panel kernel: U = P^{-1} M_KR per 128-column tile on the FP64 tensor pipe;
-//                       keeps the old rows in `cold`, writes U into rows K and U^T
-//                       into columns K (exact symmetry);
-//   3. update kernel  : lower-triangular tiles M_RR -= cold^T U, mirrored into the
-//                       upper triangle, so the matrix stays exactly symmetric and the
-//                       update costs N^2 * 128 flops instead of 2 N^2 * 128.
+// keeps M symmetric, and sweeping every block in turn yields -M^{-1}.  The symmetric sweep
+// keeps only the lower and diagonal 128-tiles current (an upper tile is read as the
+// transpose of its lower partner; get_swept does this for every reader).  Per block:
+//   1. pivot: the 128x128 block P is inverted in shared memory by Gauss-Jordan exchange
+//      with partial pivoting (local to the block); -P^{-1} goes into M_KK and P^{-1} into
+//      a scratch slot;
+//   2. row panel: per 128-column tile the old rows K (read from the lower partner for
+//      tiles right of K) are kept in `cold` and U = P^{-1} cold is computed on the FP64
+//      tensor pipe; U goes into the rows K (for tiles right of K that storage is otherwise
+//      unused and serves as this step's update operand) and U^T into the lower tiles of the
+//      columns K;
+//   3. update: lower-triangular tiles M_RR -= cold^T U, so the update costs N^2 * 128 flops
+//      instead of 2 N^2 * 128, and no tile is written twice.
+// The symmetric sweep runs steps 2-3 and the next step's pivot as one persistent launch
+// per step (sweep_step_kernel); the general sweep (matching) keeps separate row-panel,
+// column-panel and update kernels over the full matrix.
 // Total work for an N x N inverse: N^3 flops (vs 2 N^3 for a general inverse).
 #pragma once
 
