@@ -241,11 +241,16 @@ def propagate_blocks(hamiltonian, channel_blocks, Etot, radial_sectors: Sequence
         message = "Propagation produced no radial windows"
         logger.error(message)
         raise RuntimeError(message)
-    # blocks that fit the 64-wide single-block sweep (64 real rows, or 32 complex channels)
-    # go in their own batch, so that they are not padded to the larger blocks' size
-    small = 32 if config.mode == "capture" else 64
-    classes = [[g for g, b in enumerate(blocks) if len(b) <= small], [g for g, b in enumerate(blocks) if len(b) > small]]
-    if all(classes):
+    # blocks are batched by the size of their sweep matrix, so that none is padded to a larger
+    # class: 64 (the 64-wide single-block sweep: 64 real rows, or 32 complex channels), then
+    # multiples of 128 rows
+    rows = 2 if config.mode == "capture" else 1
+    def size_class(b) -> int:
+        m = rows * len(b)
+        return 64 if m <= 64 else -(-m // 128) * 128
+    keys = sorted({size_class(b) for b in blocks})
+    classes = [[g for g, b in enumerate(blocks) if size_class(b) == key] for key in keys]
+    if len(classes) > 1:
         out: list = [None] * len(blocks)
         for members in classes:
             for g, Y in zip(members, propagate_blocks(hamiltonian, tuple(blocks[g] for g in members), Etot, radial_sectors, config, window_timing=window_timing), strict=True):
