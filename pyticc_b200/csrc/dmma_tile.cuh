@@ -15,7 +15,7 @@ namespace ticc {
 constexpr size_t kTileSmemBytes = size_t(4) * kChunk * kStride * sizeof(double);  // 135168
 
 __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                : "+d"(d[0]), "+d"(d[1])
                : "d"(a), "d"(b));
 }
@@ -160,7 +160,7 @@ __device__ __forceinline__ void split_tf32(double x, unsigned& hi, unsigned& lo)
 }
 
 __device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
-  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+  asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
                : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
                : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
@@ -190,14 +190,20 @@ __device__ __forceinline__ void mma_chunk_tf32x3(TileAcc32& acc, const double* A
       split_tf32(b0[nt * 8], bh[nt][0], bl[nt][0]);
       split_tf32(b4[nt * 8], bh[nt][1], bl[nt][1]);
     }
+    // each term across the 16 accumulators before the next, so that consecutive mma are
+    // independent; every accumulator still takes lo*hi, hi*lo, hi*hi in that order
 #pragma unroll
     for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
-      for (int nt = 0; nt < 4; ++nt) {
-        mma_tf32(acc.v[mt][nt], al[mt], bh[nt][0], bh[nt][1]);
-        mma_tf32(acc.v[mt][nt], ah[mt], bl[nt][0], bl[nt][1]);
-        mma_tf32(acc.v[mt][nt], ah[mt], bh[nt][0], bh[nt][1]);
-      }
+      for (int nt = 0; nt < 4; ++nt) mma_tf32(acc.v[mt][nt], al[mt], bh[nt][0], bh[nt][1]);
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) mma_tf32(acc.v[mt][nt], ah[mt], bl[nt][0], bl[nt][1]);
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) mma_tf32(acc.v[mt][nt], ah[mt], bh[nt][0], bh[nt][1]);
   }
 }
 
@@ -556,14 +562,20 @@ __device__ __forceinline__ void mma_chunk_split(TileAcc32& acc, const unsigned* 
       bl[nt][0] = Blo[r0 + n];
       bl[nt][1] = Blo[r4 + n];
     }
+    // each term across the 16 accumulators before the next, so that consecutive mma are
+    // independent; every accumulator still takes lo*hi, hi*lo, hi*hi in that order
 #pragma unroll
     for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
-      for (int nt = 0; nt < 4; ++nt) {
-        mma_tf32(acc.v[mt][nt], al[mt], bh[nt][0], bh[nt][1]);
-        mma_tf32(acc.v[mt][nt], ah[mt], bl[nt][0], bl[nt][1]);
-        mma_tf32(acc.v[mt][nt], ah[mt], bh[nt][0], bh[nt][1]);
-      }
+      for (int nt = 0; nt < 4; ++nt) mma_tf32(acc.v[mt][nt], al[mt], bh[nt][0], bh[nt][1]);
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) mma_tf32(acc.v[mt][nt], ah[mt], bl[nt][0], bl[nt][1]);
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) mma_tf32(acc.v[mt][nt], ah[mt], bh[nt][0], bh[nt][1]);
   }
 }
 
