@@ -196,7 +196,7 @@ __device__ __forceinline__ void put_padding(double* Mb, int np, long long r, lon
 // is processed up to the end of its diagonal tile; the last pass writes Y_out's upper
 // triangle as the transpose of the lower tiles.
 constexpr int kRowCols = 4;
-__global__ void __launch_bounds__(256) ldmd_elementwise_kernel(int phase, int s, LdmdSectors sec, LdmdLayout L, const double* Yin, double* Yout) {
+__global__ void __launch_bounds__(256, 2) ldmd_elementwise_kernel(int phase, int s, LdmdSectors sec, LdmdLayout L, const double* Yin, double* Yout) {
   const int i = blockIdx.x;
   const int g = blockIdx.y;
   const int ne = L.n_energy;
@@ -249,6 +249,62 @@ __global__ void __launch_bounds__(256) ldmd_elementwise_kernel(int phase, int s,
         else wa[q] = We[j];
         if (phase == 1) wp[q] = Wep[j];
       }
+    }
+    if (!L.is_complex && (phase == 1 || phase == 2)) {
+      // the per-sector passes of a real work matrix: two energies at a time, all loads of
+      // both issued before either's stores (the stores of one energy could alias the next
+      // energy's loads as far as the compiler knows, so it would not hoist them itself)
+#pragma unroll 1
+      for (int e = 0; e < ne; e += 2) {
+        const int cnt = (ne - e < 2) ? ne - e : 2;
+        double sv[2][kRowCols], yv[2][kRowCols], y1i[2], y2i[2];
+        double* Mv[2];
+        const double* y2row[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int b = g * ne + e + (u < cnt ? u : 0);
+          Mv[u] = L.M + (long long)b * np * np;
+          const double* y1 = L.y1 + ((long long)(phase == 1 ? s - 1 : s) * batch + b) * n;
+          y2row[u] = L.y2 + ((long long)(phase == 1 ? s - 1 : s) * batch + b) * n;
+          y1i[u] = y1[i];
+          y2i[u] = y2row[u][i];
+#pragma unroll
+          for (int q = 0; q < kRowCols; ++q) {
+            const int j = j0 + q * 256 + threadIdx.x;
+            sv[u][q] = yv[u][q] = 0.0;
+            if (j < n && j < jlim) {
+              sv[u][q] = Mv[u][(long long)i * np + j];
+              yv[u][q] = y2row[u][j];
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          if (u >= cnt) break;
+          const int b = g * ne + e + u;
+          const double* y1c = L.y1 + ((long long)s * batch + b) * n;  // this sector's y1 (phase 1)
+          const double y1cur = y1c[i];
+#pragma unroll
+          for (int q = 0; q < kRowCols; ++q) {
+            const int j = j0 + q * 256 + threadIdx.x;
+            if (j >= jlim) continue;
+            if (j >= n) {  // padding column
+              put_padding(Mv[u], np, i, j);
+              continue;
+            }
+            const double d = (i == j) ? 1.0 : 0.0;
+            double x;
+            if (phase == 1) {
+              x = hp * (wp[q] - d * ref_p) / 3.0 + d * y1i[u] + y2i[u] * sv[u][q] * yv[u][q];
+              x += h * (wa[q] - d * ref) / 3.0 + d * y1cur;
+            } else {
+              x = 2.0 * wa[q] + 2.0 * d * y1i[u] + y2i[u] * sv[u][q] * yv[u][q];
+            }
+            Mv[u][(long long)i * np + j] = x;
+          }
+        }
+      }
+      continue;
     }
 #pragma unroll 1
     for (int e = 0; e < ne; ++e) {
