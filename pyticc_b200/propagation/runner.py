@@ -227,6 +227,20 @@ def blocks_window(n_channel: int, n_block: int, n_sector: int) -> int:
     return max(1, min(n_sector, MAX_SECTORS_PER_WINDOW, WINDOW_BYTES // per_sector, 65535 // n_block))
 
 
+def block_size_classes(blocks, mode: str) -> list[list[int]]:
+    """Positions of the blocks grouped by the size of their sweep matrix, smallest first, so
+    that no block is padded to a larger class: 64 rows (the 64-wide single-block sweep: 64
+    real channels, or 32 complex ones in capture mode), then multiples of 128 rows."""
+    rows = 2 if mode == "capture" else 1
+
+    def size_class(b) -> int:
+        m = rows * len(b)
+        return 64 if m <= 64 else -(-m // 128) * 128
+
+    keys = sorted({size_class(b) for b in blocks})
+    return [[g for g, b in enumerate(blocks) if size_class(b) == key] for key in keys]
+
+
 def propagate_blocks(hamiltonian, channel_blocks, Etot, radial_sectors: Sequence[RadialSector], config: Propagation, *, window_timing: list | None = None) -> tuple[torch.Tensor, ...]:
     """Y at the last sector end of every channel block, one (n_energy, n_b, n_b) device
     tensor per block (reference runner.py:165-322).  All blocks share each radial window
@@ -241,15 +255,7 @@ def propagate_blocks(hamiltonian, channel_blocks, Etot, radial_sectors: Sequence
         message = "Propagation produced no radial windows"
         logger.error(message)
         raise RuntimeError(message)
-    # blocks are batched by the size of their sweep matrix, so that none is padded to a larger
-    # class: 64 (the 64-wide single-block sweep: 64 real rows, or 32 complex channels), then
-    # multiples of 128 rows
-    rows = 2 if config.mode == "capture" else 1
-    def size_class(b) -> int:
-        m = rows * len(b)
-        return 64 if m <= 64 else -(-m // 128) * 128
-    keys = sorted({size_class(b) for b in blocks})
-    classes = [[g for g, b in enumerate(blocks) if size_class(b) == key] for key in keys]
+    classes = block_size_classes(blocks, config.mode)
     if len(classes) > 1:
         out: list = [None] * len(blocks)
         for members in classes:

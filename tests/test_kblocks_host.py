@@ -127,3 +127,15 @@ def test_oracle_block_solve_matches_reference(name):
             n = s.shape[0]
             assert n == g[f"b{b}_n_open"][e]
             np.testing.assert_allclose(s, g[f"b{b}_Smat"][e, :n, :n], rtol=1e-10, atol=1e-10)
+
+
+def test_blocks_are_batched_by_sweep_size():
+    from pyticc_b200.propagation.runner import block_size_classes
+
+    sizes = [4, 64, 65, 128, 129, 200, 360, 30, 300]
+    blocks = [tuple(range(n)) for n in sizes]
+    assert block_size_classes(blocks, "inelastic") == [[0, 1, 7], [2, 3], [4, 5], [6, 8]]
+    # capture mode sweeps the 2n x 2n real embedding
+    assert block_size_classes(blocks, "capture") == [[0, 7], [1], [2, 3], [4], [5], [8], [6]]
+    assert block_size_classes([tuple(range(10))], "inelastic") == [[0]]
+
