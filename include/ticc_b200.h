@@ -14,7 +14,9 @@
  * {code, batch item, detail, 0}.  Codes: 0 ok, 1 singular pivot block in a
  * symmetric sweep (detail = block index), 2 non-finite output, 3 Bessel continued
  * fraction did not converge (detail = channel), 4 energy exactly at a threshold,
- * 5 more open channels than the caller's max_open.
+ * 5 more open channels than the caller's max_open, 6 a step of a symmetric sweep
+ * gave up waiting for a row-panel tile of its own launch (an internal error; the
+ * wait is bounded, the results of that call are invalid).
  *
  * Matrices are row-major float64, or complex128 with interleaved (re, im) pairs
  * when `is_complex` is set.  Symmetric inputs are required where noted: their
