@@ -76,7 +76,8 @@ int ticc_sym_inverse(void* M, int n, int batch, int is_complex, void* workspace,
  * a device looks up the array's device address (cudaGetSymbolAddress) with that device
  * current; make that first call before any stream capture.  All calls on a device share
  * the one array: calls that overlap on the GPU (different streams, or threads) race and
- * must be serialised by the caller.  No part of the array needs clearing between calls. */
+ * must be serialised by the caller.  The caller clears nothing: each call zeroes the words
+ * of the array that must start at zero (the sweep's work queues and tile flags) itself. */
 int ticc_sym_inverse_noalloc(void* M, int n, int batch, int is_complex, int* device_status, void* stream);
 
 /* ---- LDMD propagation -------------------------------------------------------
@@ -94,11 +95,12 @@ int ticc_sym_inverse_noalloc(void* M, int n, int batch, int is_complex, int* dev
  *              for element (i, j); ticc_contract's W assembly produces such matrices), at
  *              the given element stride between consecutive sectors (e.g. 2*n*n for an
  *              interleaved point list).
- *   precision  TICC_PRECISION_FP64 (all-FP64) or TICC_PRECISION_MIXED: the trailing
- *              updates of the leading sweep blocks whose channels are all closed with a
- *              local wavenumber above 30 bohr^-1 at the batch's highest energy run as an
- *              FP32-accurate TF32x3 product; pivots, panels, open blocks, Q_mid and the Y
- *              recurrence stay FP64.  Order channels most-closed first to benefit. */
+ *   precision  TICC_PRECISION_FP64 (all-FP64) or TICC_PRECISION_MIXED: the sweep steps
+ *              over the leading blocks whose channels are all closed with a local
+ *              wavenumber above 30 bohr^-1 at the batch's highest energy take an
+ *              FP32-accurate TF32x3 product for their row panel and trailing update;
+ *              pivot inversions, the open blocks' steps, Q_mid and the Y recurrence stay
+ *              FP64.  Order channels most-closed first to benefit. */
 int ticc_ldmd_workspace_size(int n_channel, int n_energy, int n_sector, int is_complex, int precision, size_t* bytes);
 int ticc_ldmd_propagate(void* Y, int is_complex, const double* energies, int n_energy, double reduced_mass, const double* half_steps,
                         const double* W_start, long long W_start_stride, const double* W_mid, long long W_mid_stride, const double* W_end,
