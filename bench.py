@@ -38,7 +38,7 @@ def parse_args():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["native", "reference"], default="native")
-    p.add_argument("--batch", type=int, default=16, help="energies per step")
+    p.add_argument("--batch", type=int, default=32, help="energies per step (per solve call); 256 / batch batches per parity block")
     p.add_argument("--precision", choices=["fp64", "mixed"], default="mixed", help="headline arm precision")
     p.add_argument("--schedule", choices=["fixed", "learned"], default="learned", help="headline arm sector schedule")
     p.add_argument("--plain-steps", type=int, default=None, help="timed steps of the plain FP64 fixed-step arm (default: steps - 1, at least 1)")
