@@ -267,26 +267,6 @@ __device__ __forceinline__ void acc32_to_smem_mirror(const TileAcc32& acc, doubl
       }
 }
 
-__device__ __forceinline__ void acc32_to_smem(const TileAcc32& acc, double* Cs, double scale) {
-  const int tid = threadIdx.x;
-  const int warp = tid >> 5;
-  const int lane = tid & 31;
-  const int wm = (warp >> 2) * 64;
-  const int wn = (warp & 3) * 32;
-  const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-  for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-    for (int nt = 0; nt < 4; ++nt) {
-      const int row = wm + mt * 16 + g;
-      const int col = wn + nt * 8 + 2 * t;
-      Cs[row * kStride + col] = scale * acc.v[mt][nt][0];
-      Cs[row * kStride + col + 1] = scale * acc.v[mt][nt][1];
-      Cs[(row + 8) * kStride + col] = scale * acc.v[mt][nt][2];
-      Cs[(row + 8) * kStride + col + 1] = scale * acc.v[mt][nt][3];
-    }
-}
-
 // ---- trailing-update tile with the C tile staged during the product ----------------------
 // The update M_tile -= A^T B of the sweep reads the 128 x 128 FP64 tile of M once; here it
 // is copied into shared memory by cp.async while the first K-chunk is multiplied, so the
@@ -382,12 +362,9 @@ __device__ inline void tile_update_product(Acc& acc, const double* A, long long 
   update_mainloop(acc, A, lda, B, ldb, K, stages);
 }
 
-// Epilogue of an update tile: Cs[row][col] -= acc in the accumulator's own fragment layout
-// and, for an off-diagonal tile of the symmetric sweep (`mirror`), the new value also goes
-// straight from registers to its transposed position M[c0 + col][r0 + row] of Mt (= M at
-// row c0, column r0): the 8 lanes sharing a column write 8 consecutive rows, i.e. whole 64-byte
-// segments, so the transpose needs no conflicting column reads of shared memory.
-__device__ __forceinline__ void acc_sub_smem(const TileAcc& acc, double* Cs, double* Mt, long long ld, bool mirror) {
+// Cs[row][col] -= acc in the accumulator's own fragment layout (the pivot tile of a fused
+// next-pivot update, inverted in shared memory afterwards).
+__device__ __forceinline__ void acc_sub_smem(const TileAcc& acc, double* Cs) {
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
   const int lane = tid & 31;
@@ -399,16 +376,11 @@ __device__ __forceinline__ void acc_sub_smem(const TileAcc& acc, double* Cs, dou
     for (int nt = 0; nt < 4; ++nt) {
       const int row = wm + mt * 8 + (lane >> 2), col = wn + nt * 8 + 2 * (lane & 3);
       double* d = Cs + row * kStride + col;
-      const double v0 = d[0] - acc.v[mt][nt][0], v1 = d[1] - acc.v[mt][nt][1];
-      d[0] = v0;
-      d[1] = v1;
-      if (mirror) {
-        Mt[(long long)col * ld + row] = v0;
-        Mt[(long long)(col + 1) * ld + row] = v1;
-      }
+      d[0] -= acc.v[mt][nt][0];
+      d[1] -= acc.v[mt][nt][1];
     }
 }
-__device__ __forceinline__ void acc_sub_smem(const TileAcc32& acc, double* Cs, double* Mt, long long ld, bool mirror) {
+__device__ __forceinline__ void acc_sub_smem(const TileAcc32& acc, double* Cs) {
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
   const int lane = tid & 31;
@@ -423,13 +395,8 @@ __device__ __forceinline__ void acc_sub_smem(const TileAcc32& acc, double* Cs, d
       for (int h = 0; h < 2; ++h) {
         const int row = wm + mt * 16 + g + 8 * h, col = wn + nt * 8 + 2 * t;
         double* d = Cs + row * kStride + col;
-        const double v0 = d[0] - acc.v[mt][nt][2 * h], v1 = d[1] - acc.v[mt][nt][2 * h + 1];
-        d[0] = v0;
-        d[1] = v1;
-        if (mirror) {
-          Mt[(long long)col * ld + row] = v0;
-          Mt[(long long)(col + 1) * ld + row] = v1;
-        }
+        d[0] -= acc.v[mt][nt][2 * h];
+        d[1] -= acc.v[mt][nt][2 * h + 1];
       }
 }
 

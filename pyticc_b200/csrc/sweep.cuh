@@ -375,34 +375,16 @@ __device__ inline void load_cold_tile(double* Cb, int ld, const double* Mb, int 
   }
 }
 
-// Write a finished 128x128 tile from shared memory to M at (r0, c0).  With `mirror`
-// (symmetric sweep) its transpose also goes to (c0, r0) and a diagonal tile is written
-// symmetrised from its lower half.
-__device__ inline void store_tile(double* Mb, int ld, int r0, int c0, const double* Cs, bool mirror) {
+// Write a finished 128x128 tile from shared memory to M at (r0, c0).
+__device__ inline void store_tile(double* Mb, int ld, int r0, int c0, const double* Cs) {
   const int tid = threadIdx.x;
-  const bool diagonal = mirror && (r0 == c0);
   for (int piece = tid; piece < kBlock * 64; piece += kGemmThreads) {
     const int r = piece >> 6;
     const int c = (piece & 63) * 2;
     double2 v;
-    if (diagonal) {
-      v.x = (r >= c) ? Cs[r * kStride + c] : Cs[c * kStride + r];
-      v.y = (r >= c + 1) ? Cs[r * kStride + c + 1] : Cs[(c + 1) * kStride + r];
-    } else {
-      v.x = Cs[r * kStride + c];
-      v.y = Cs[r * kStride + c + 1];
-    }
+    v.x = Cs[r * kStride + c];
+    v.y = Cs[r * kStride + c + 1];
     *reinterpret_cast<double2*>(Mb + (long long)(r0 + r) * ld + c0 + c) = v;
-  }
-  if (mirror && !diagonal) {
-    for (int piece = tid; piece < kBlock * 64; piece += kGemmThreads) {
-      const int r = piece >> 6;        // destination row offset (a column of Cs)
-      const int c = (piece & 63) * 2;  // destination column offset (a row of Cs)
-      double2 v;
-      v.x = Cs[c * kStride + r];
-      v.y = Cs[(c + 1) * kStride + r];
-      *reinterpret_cast<double2*>(Mb + (long long)(c0 + r) * ld + r0 + c) = v;
-    }
   }
 }
 
@@ -427,7 +409,7 @@ __global__ void __launch_bounds__(kGemmThreads) sweep_rowpanel_kernel(double* __
   // the otherwise unused upper tile, read by this step's update) from shared memory
   acc_to_smem_mirror(acc, smem, Mb + (long long)c0 * ld + k0, ld, kSym && jt > kb);
   __syncthreads();
-  store_tile(Mb, ld, k0, c0, smem, false);
+  store_tile(Mb, ld, k0, c0, smem);
   if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) *queue = 0;  // the step's update tile queue
 }
 
@@ -457,7 +439,7 @@ __global__ void __launch_bounds__(kGemmThreads) sweep_colpanel_kernel(double* __
   tile_gemm_tn(acc, Cb + r0, ld, pinv + (long long)b * 2 * kBlock * kBlock, kBlock, kBlock, smem);
   acc_to_smem(acc, smem, 1.0);
   __syncthreads();
-  store_tile(Mb, ld, r0, k0, smem, false);
+  store_tile(Mb, ld, r0, k0, smem);
 }
 
 __device__ __forceinline__ void lower_pair(int idx, int& a, int& b) {
@@ -624,11 +606,11 @@ __global__ void __launch_bounds__(kGemmThreads, 1) sweep_update_kernel(double* _
     if (reduced) {
       TileAcc32 acc;
       tile_update_product(acc, A, ld, B, ld, kBlock, smem, Cs, Cg, ld);
-      acc_sub_smem(acc, Cs, Mb, ld, false);
+      acc_sub_smem(acc, Cs);
     } else {
       TileAcc acc;
       tile_update_product(acc, A, ld, B, ld, kBlock, smem, Cs, Cg, ld);
-      acc_sub_smem(acc, Cs, Mb, ld, false);
+      acc_sub_smem(acc, Cs);
     }
     __syncthreads();
     if (kSym) {  // symmetrise the pivot block from its lower half, as store_tile would
@@ -709,7 +691,7 @@ __device__ inline void rowpanel_unit(double* Mb, int ld, int kb, int jt, const d
     acc_to_smem_mirror(acc, smem, Mb + (long long)c0 * ld + k0, ld, jt > kb);
   }
   __syncthreads();
-  store_tile(Mb, ld, k0, c0, smem, false);
+  store_tile(Mb, ld, k0, c0, smem);
 }
 
 template <class Acc>
@@ -778,11 +760,11 @@ __global__ void __launch_bounds__(kGemmThreads, 1) sweep_step_kernel(double* __r
       if (reduced) {
         TileAcc32 acc;
         tile_update_product(acc, A, ld, B, ld, kBlock, smem, Cs, Cg, ld);
-        acc_sub_smem(acc, Cs, Mb, ld, false);
+        acc_sub_smem(acc, Cs);
       } else {
         TileAcc acc;
         tile_update_product(acc, A, ld, B, ld, kBlock, smem, Cs, Cg, ld);
-        acc_sub_smem(acc, Cs, Mb, ld, false);
+        acc_sub_smem(acc, Cs);
       }
       __syncthreads();
       for (int e = tid; e < kBlock * kBlock; e += kGemmThreads) {  // symmetrise from the lower half
