@@ -412,7 +412,16 @@ def run_blocks(args, rank, world, local):
         energies = wl.energies[energy_slice]
         sectors = sectors_of[block_index]
         kb = k_blocks[block_index]
-        Ys = runner.propagate_blocks(ham, tuple(b.channel_indices for b in kb), energies, sectors, config, window_timing=windows)
+        # the size classes run concurrently on their own streams, so the roofline takes the
+        # whole propagation on the caller's stream (after the join), not the sum of windows
+        inner = None if windows is None else []
+        if windows is not None:
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record()
+        Ys = runner.propagate_blocks(ham, tuple(b.channel_indices for b in kb), energies, sectors, config, window_timing=inner)
+        if windows is not None:
+            t1.record()
+            windows.append((t0, t1, sum(f for _, _, f in inner)))
         return [scattering.finalize_K_block(wl.system.basis, b, Y, energies, ham.reduced_mass, sectors[-1].radial_end, approx=wl.system.approx) for b, Y in zip(kb, Ys, strict=True)]
 
     for k in range(args.warmup):

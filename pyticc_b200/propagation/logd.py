@@ -85,10 +85,11 @@ def propagate_device(Y: torch.Tensor, energies: torch.Tensor, reduced_mass: floa
     return Y
 
 
-def propagate_blocks_device(Y: torch.Tensor, energies: torch.Tensor, reduced_mass: float, half_steps: torch.Tensor, W_start: torch.Tensor, W_mid: torch.Tensor, W_end: torch.Tensor, *, stride, block_stride: int, precision: int = nat.PRECISION_FP64) -> torch.Tensor:
+def propagate_blocks_device(Y: torch.Tensor, energies: torch.Tensor, reduced_mass: float, half_steps: torch.Tensor, W_start: torch.Tensor, W_mid: torch.Tensor, W_end: torch.Tensor, *, stride, block_stride: int, precision: int = nat.PRECISION_FP64, workspace_slot: int = 0) -> torch.Tensor:
     """Propagate device-resident Y of shape (n_block, n_energy, n, n) in place: block g
     reads its W at element offset g * block_stride from the three W views, whose
-    consecutive sectors are ``stride`` elements apart."""
+    consecutive sectors are ``stride`` elements apart.  Calls that may run concurrently on
+    different streams pass different ``workspace_slot``s."""
     lib = nat.load_library()
     n_block, n_energy, n, _ = Y.shape
     n_sector = half_steps.numel()
@@ -96,7 +97,7 @@ def propagate_blocks_device(Y: torch.Tensor, energies: torch.Tensor, reduced_mas
     dev = Y.device
     with torch.cuda.device(dev):
         nbytes = nat.size_query(lib.ticc_ldmd_blocks_workspace_size, n, n_energy, n_block, n_sector, is_complex, precision)
-        work = nat.Workspace.get(dev, nbytes)
+        work = nat.Workspace.get(dev, nbytes, slot=workspace_slot)
         status = nat.DeviceStatus(dev)
         nat.check(
             lib.ticc_ldmd_propagate_blocks(

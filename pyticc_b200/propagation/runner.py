@@ -10,6 +10,7 @@ Y stays on the device for the whole traversal.  Windows are sized by device memo
 from __future__ import annotations
 
 from collections.abc import Sequence
+from concurrent.futures import ThreadPoolExecutor
 from math import ceil
 from time import perf_counter
 
@@ -149,6 +150,7 @@ def propagate(hamiltonian, Etot, radial_sectors: Sequence[RadialSector], config:
 
 # ---- several channel blocks (coupled states, NNCC) -------------------------------------------
 DUMMY_P2 = 3600.0  # local wavenumber^2 (bohr^-2) of the closed channels that pad a smaller block
+CLASS_WORKSPACE_SLOT = 16  # first workspace slot of the concurrently propagated size classes
 
 
 class DeviceBlocks:
@@ -241,10 +243,12 @@ def block_size_classes(blocks, mode: str) -> list[list[int]]:
     return [[g for g, b in enumerate(blocks) if size_class(b) == key] for key in keys]
 
 
-def propagate_blocks(hamiltonian, channel_blocks, Etot, radial_sectors: Sequence[RadialSector], config: Propagation, *, window_timing: list | None = None) -> tuple[torch.Tensor, ...]:
+def propagate_blocks(hamiltonian, channel_blocks, Etot, radial_sectors: Sequence[RadialSector], config: Propagation, *, window_timing: list | None = None, workspace_slot: int = 0) -> tuple[torch.Tensor, ...]:
     """Y at the last sector end of every channel block, one (n_energy, n_b, n_b) device
-    tensor per block (reference runner.py:165-322).  All blocks share each radial window
-    and advance together in one batched LDMD call per window."""
+    tensor per block (reference runner.py:165-322).  All blocks of a size class share each
+    radial window and advance together in one batched LDMD call per window; the size
+    classes run concurrently, each on its own CUDA stream (host thread), so that a small
+    class fills the SMs a larger one leaves idle."""
     energies_np = get_Etot(Etot)
     blocks = tuple(tuple(int(i) for i in b) for b in channel_blocks)
     if not blocks or any(not b for b in blocks):
@@ -257,9 +261,23 @@ def propagate_blocks(hamiltonian, channel_blocks, Etot, radial_sectors: Sequence
         raise RuntimeError(message)
     classes = block_size_classes(blocks, config.mode)
     if len(classes) > 1:
+        dev = resolve_device(config.device)
+        main = torch.cuda.current_stream(dev)
+        streams = [torch.cuda.Stream(dev) for _ in classes]
+
+        def run(k: int):
+            streams[k].wait_stream(main)
+            with torch.cuda.device(dev), torch.cuda.stream(streams[k]):
+                members = tuple(blocks[g] for g in classes[k])
+                return propagate_blocks(hamiltonian, members, Etot, radial_sectors, config, window_timing=window_timing, workspace_slot=CLASS_WORKSPACE_SLOT + k)
+
+        with ThreadPoolExecutor(max_workers=len(classes)) as pool:
+            results = list(pool.map(run, range(len(classes))))
         out: list = [None] * len(blocks)
-        for members in classes:
-            for g, Y in zip(members, propagate_blocks(hamiltonian, tuple(blocks[g] for g in members), Etot, radial_sectors, config, window_timing=window_timing), strict=True):
+        for k, members in enumerate(classes):
+            main.wait_stream(streams[k])
+            for g, Y in zip(members, results[k], strict=True):
+                Y.record_stream(main)  # made on the class's stream, used on the caller's
                 out[g] = Y
         return tuple(out)
     dev = resolve_device(config.device)
@@ -294,7 +312,7 @@ def propagate_blocks(hamiltonian, channel_blocks, Etot, radial_sectors: Sequence
         if window_timing is not None:
             t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             t0.record()
-        propagate_blocks_device(Y, energies, db.reduced_mass, halves, W[0, 0], W[0, 1], W[0, 2], stride=(stride, stride, stride), block_stride=points_max * n * n, precision=precision)
+        propagate_blocks_device(Y, energies, db.reduced_mass, halves, W[0, 0], W[0, 1], W[0, 2], stride=(stride, stride, stride), block_stride=points_max * n * n, precision=precision, workspace_slot=workspace_slot)
         if window_timing is not None:
             t1.record()
             window_timing.append((t0, t1, flops_per_unit * len(window) * energies.numel()))
