@@ -366,7 +366,7 @@ def main():
             "unit": "TFLOP/s",
             "frac": achieved / peak if achieved and peak else None,
             "traffic": None,
-            "kernel": "ticc_ldmd_propagate of the headline arm (batched symmetric sweeps; FP64 DMMA, TF32x3 on strongly closed blocks in mixed precision); peak = cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)",
+            "kernel": "ticc_ldmd_propagate of the headline arm (batched symmetric sweeps; FP64 DMMA, TF32x3 on strongly closed blocks in mixed precision); peak = cuBLAS DGEMM 8192^3 measured in this run (no measured FP64 peak is supplied)",
             "flops_per_unit": f"2 N^3 per (sector, energy), N={n_channel}, counted in FP64-equivalent flops",
         },
         "cpu_baseline": cpu,

@@ -179,7 +179,7 @@ int ticc_match_smatrix(const void* Y, int is_complex, double Rmatch, const doubl
  * build_radial_sectors (propagation/grid.py:193-239) only.  A small MLP proposes, per
  * fixed-step sector, log2 of how many aligned sectors may be merged into one; merged
  * sectors keep their start/mid/end points on the same grid, so the PotentialGrid is
- * unchanged.  The fixed-step propagation stays the judge of every learned schedule.
+ * unchanged.  Every learned schedule is checked against the fixed-step propagation.
  *
  * Network: n_feature -> n_hidden (tanh) -> n_hidden (tanh) -> 1, FP32 parameters packed as
  * W1[n_hidden][n_feature], b1, W2[n_hidden][n_hidden], b2, w3[n_hidden], b3. */

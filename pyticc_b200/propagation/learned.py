@@ -17,7 +17,7 @@ no PES is evaluated anywhere new.
                            |p| h below 2.8 for every open channel (the reference
                            propagators cot/csc of an LDMD sector have poles at
                            |p| h = n pi; the cap keeps merged sectors below the first)
-* ``validate_learned``     the fixed-step solve judges the learned one: accepted only if
+* ``validate_learned``     the fixed-step solve checks the learned one: accepted only if
                            max|dS| is within tolerance and the open-channel counts agree.
 """
 

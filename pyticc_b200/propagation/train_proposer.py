@@ -5,7 +5,7 @@
 Training labels come from step doubling with the plain FP64 propagator on three systems
 of the shapes this library is benchmarked on (the rigid-rotor A+BC block, the vibrating
 Morse A+BC block at J=30, and ultracold capture at J=10), at the lowest and highest
-energy of each range.  The fitted network is then judged by the fixed-step solve on
+energy of each range.  The fitted network is then checked against the fixed-step solve on
 held-out energies of every system (max|dS| and the sector counts are reported).
 """
 
