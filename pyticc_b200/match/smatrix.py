@@ -77,5 +77,12 @@ def get_Smat(Ymat, Rmatch: float, Etot, reduced_mass: float, E_int, L) -> tuple[
     complex_mode = Ymat.is_complex() if isinstance(Ymat, torch.Tensor) else np.iscomplexobj(np.asarray(Ymat))
     Y = nat.as_device(Ymat, dev, torch.complex128 if complex_mode else torch.float64)
     S, n_open = get_Smat_device(Y, Rmatch, energies, reduced_mass, E_int_a, L_a)
-    S_host = S.cpu().numpy()
-    return tuple(np.ascontiguousarray(S_host[e, : n_open[e], : n_open[e]]) for e in range(energies.size))
+    return open_blocks_to_host(S, n_open)
+
+
+def open_blocks_to_host(S: torch.Tensor, n_open: np.ndarray) -> tuple[np.ndarray, ...]:
+    """Host copies of the open-open blocks of a device S batch; only the leading
+    max(n_open) x max(n_open) corner of each matrix crosses to the host."""
+    m = int(np.max(n_open)) if len(n_open) else 0
+    S_host = S[:, :m, :m].cpu().numpy()
+    return tuple(np.ascontiguousarray(S_host[e, : n_open[e], : n_open[e]]) for e in range(len(n_open)))

@@ -19,7 +19,7 @@ from .. import _native as nat
 from ..basis import gauss_legendre_dvr, get_Umat_BF
 from ..energy import get_Etot
 from ..match.asymptotic import get_Bmat_BF_to_SF, transform_device
-from ..match.smatrix import get_Smat_device
+from ..match.smatrix import get_Smat_device, open_blocks_to_host
 from ..matrix.interaction import DeviceBasisCache, VBasisBF, contract_device, prepare_atom_diatom, prepare_diatom_diatom
 from ..pes import PESWrapper, get_Vgrid_atom_diatom, get_Vgrid_diatom_diatom
 from ..propagation.config import Propagation
@@ -234,8 +234,7 @@ def _match(Y: torch.Tensor, B: np.ndarray, L: np.ndarray, E_int: np.ndarray, Rma
     """BF -> SF transform and matching on the device; one open-open S per energy."""
     Y_sf = transform_device(Y, nat.as_device(B, Y.device, torch.float64))
     S, n_open = get_Smat_device(Y_sf, Rmatch, energies, reduced_mass, E_int, L)
-    S_host = S.cpu().numpy()
-    return tuple(np.ascontiguousarray(S_host[e, : n_open[e], : n_open[e]]) for e in range(energies.size))
+    return open_blocks_to_host(S, n_open)
 
 
 def finalize_K_block(basis, block: KBlock, Y_BF: torch.Tensor, Etot, reduced_mass: float, Rmatch: float, *, approx: Approx = Approx.NNCC) -> KBlockResult:
