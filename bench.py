@@ -29,6 +29,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "S-matrix solves/s on 1 B200: mixed+learned vs plain FP64 LogD at max|dS|<=1e-6"
+STEP_KERNEL_DRAM_BYTES = 342_238_208 + 278_014_208  # ncu: one FP64 sweep step launch, 16 matrices of 2048^2
 WORKLOAD = "vibrating A+BC exact CC: Morse diatom v<=3 j<=30, J=30, both parities (N=1984/1860), 938 LDMD sectors 2.5-40 bohr h=0.02, 256 energies 100-3000 cm^-1"
 
 
@@ -365,7 +366,10 @@ def main():
             "peak": peak,
             "unit": "TFLOP/s",
             "frac": achieved / peak if achieved and peak else None,
-            "traffic": None,
+            # DRAM bytes per launch of the dominant kernel (sweep_step_kernel, one sweep step of
+            # 16 matrices of 2048^2) from one ncu capture; the algorithmic bytes are 595 MB
+            "traffic": STEP_KERNEL_DRAM_BYTES,
+            "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one sweep_step_kernel launch (ncu capture, 16 matrices of 2048^2, 342 + 278 MB); algorithmic 595 MB",
             "kernel": "ticc_ldmd_propagate of the headline arm (batched symmetric sweeps; FP64 DMMA, TF32x3 on strongly closed blocks in mixed precision); peak = cuBLAS DGEMM 8192^3 measured in this run (no measured FP64 peak is supplied)",
             "flops_per_unit": f"2 N^3 per (sector, energy), N={n_channel}, counted in FP64-equivalent flops",
         },
