@@ -368,8 +368,8 @@ def main():
             "frac": achieved / peak if achieved and peak else None,
             # DRAM bytes per launch of the dominant kernel (sweep_step_kernel, one sweep step of
             # 16 matrices of 2048^2) from one ncu capture; the algorithmic bytes are 595 MB
-            "traffic": STEP_KERNEL_DRAM_BYTES,
-            "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one sweep_step_kernel launch (ncu capture, 16 matrices of 2048^2, 342 + 278 MB); algorithmic 595 MB",
+            "traffic": STEP_KERNEL_DRAM_BYTES * args.batch / 16,
+            "traffic_note": f"dram__bytes_read.sum + dram__bytes_write.sum of one sweep_step_kernel launch from an ncu capture of 16 matrices of 2048^2 (342 + 278 MB, algorithmic 595 MB), scaled to the {args.batch} matrices of a launch here (the traffic is per matrix)",
             "kernel": "ticc_ldmd_propagate of the headline arm (batched symmetric sweeps; FP64 DMMA, TF32x3 on strongly closed blocks in mixed precision); peak = cuBLAS DGEMM 8192^3 measured in this run (no measured FP64 peak is supplied)",
             "flops_per_unit": f"2 N^3 per (sector, energy), N={n_channel}, counted in FP64-equivalent flops",
         },
