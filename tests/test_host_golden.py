@@ -108,3 +108,20 @@ def test_validation_errors_match_reference():
         tb.get_Etot([[1.0]])
     with pytest.raises(ValueError, match="At least one total energy"):
         tb.get_Etot([])
+
+
+def test_open_blocks_to_host_copies_only_the_open_corner():
+    """The host copy of a matched batch keeps each energy's open-open block (in the
+    reference's order) and nothing beyond the largest one."""
+    import torch
+
+    from pyticc_b200.match.smatrix import open_blocks_to_host
+
+    rng = np.random.default_rng(7)
+    S = torch.as_tensor(rng.normal(size=(3, 6, 6)) + 1j * rng.normal(size=(3, 6, 6)))
+    n_open = np.array([2, 0, 4])
+    out = open_blocks_to_host(S, n_open)
+    assert [o.shape for o in out] == [(2, 2), (0, 0), (4, 4)]
+    for e, o in enumerate(out):
+        np.testing.assert_array_equal(o, S[e, : n_open[e], : n_open[e]].numpy())
+    assert [o.shape for o in open_blocks_to_host(S[:1], np.array([0]))] == [(0, 0)]
