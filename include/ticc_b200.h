@@ -66,9 +66,8 @@ int ticc_sym_inverse_workspace_size(int n, int batch, int is_complex, size_t* by
 int ticc_sym_inverse(void* M, int n, int batch, int is_complex, void* workspace, size_t workspace_bytes, int* device_status, void* stream);
 
 /* Allocation-free variant of ticc_sym_inverse, for callers that cannot allocate device
- * memory: code running while a stream is captured into a CUDA graph (no cudaMalloc
- * there), plugin hosts that pass only buffers they own, and C/Fortran drivers without a
- * device allocator.  It has no counterpart in the reference.  Scratch comes from a fixed
+ * memory: plugin hosts that pass only buffers they own, runtimes that fix their device
+ * memory budget at start-up, and C/Fortran drivers without a device allocator.  It has no counterpart in the reference.  Scratch comes from a fixed
  * 32 MiB device array inside the library (held by every GPU that loads it until the
  * process exits), so batch * (Np^2 + 128 Np + 32784) doubles must fit in 32 MiB, with
  * Np = n (2n when complex) rounded up to 128 — e.g. n <= 512 with batch <= 11; larger
@@ -79,6 +78,14 @@ int ticc_sym_inverse(void* M, int n, int batch, int is_complex, void* workspace,
  * must be serialised by the caller.  The caller clears nothing: each call zeroes the words
  * of the array that must start at zero (the sweep's work queues and tile flags) itself. */
 int ticc_sym_inverse_noalloc(void* M, int n, int batch, int is_complex, int* device_status, void* stream);
+
+/* Test hook with no counterpart in the reference: the number of polls a wait of the fused
+ * sweep step (a tile waiting for the row-panel tiles it reads) may spend before it gives
+ * up, raises the call's abort flag and reports device status 6 (the default, 2^22 polls,
+ * is restored by passing 4194304).  0 makes every wait give up before its first poll, so a
+ * test can check the bounded-wait path; the kernel then finishes without the skipped work
+ * and the context stays usable.  Applies to the current device. */
+int ticc_debug_set_step_poll_limit(long long polls);
 
 /* ---- LDMD propagation -------------------------------------------------------
  * Propagate n_energy log-derivative matrices Y through n_sector Manolopoulos LDMD
@@ -106,6 +113,16 @@ int ticc_ldmd_propagate(void* Y, int is_complex, const double* energies, int n_e
                         const double* W_start, long long W_start_stride, const double* W_mid, long long W_mid_stride, const double* W_end,
                         long long W_end_stride, int n_sector, int n_channel, int precision, void* workspace, size_t workspace_bytes,
                         int* device_status, void* stream);
+
+/* Diagnostic with no counterpart in the reference: after a mixed-precision
+ * ticc_ldmd_propagate / ticc_ldmd_propagate_blocks call, the number of leading 128-wide
+ * sweep blocks of each sector that took the TF32x3 product (both sweeps of a sector use
+ * the same count), copied from the call's workspace into the HOST array counts[n_sector]
+ * in stream order (enqueue it on the propagation's stream before the workspace is reused;
+ * with pinned memory the copy is asynchronous: synchronise before reading counts).  Pass
+ * the same sizes as the propagation call. */
+int ticc_ldmd_reduced_blocks(const void* workspace, size_t workspace_bytes, int n_channel, int n_energy, int n_block, int n_sector, int is_complex,
+                             int precision, int* counts, void* stream);
 
 /* Several channel blocks through the same sectors in one call: the coupled-states and
  * NNCC K blocks of one (J, parity) system.  Replaces the per-block loop of

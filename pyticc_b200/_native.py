@@ -48,8 +48,10 @@ SIGNATURES: dict[str, tuple[list, type]] = {
     "ticc_sym_inverse_workspace_size": ([_I, _I, _I, _PSZ], _I),
     "ticc_sym_inverse": ([_P, _I, _I, _I, _P, _SZ, _P, _P], _I),
     "ticc_sym_inverse_noalloc": ([_P, _I, _I, _I, _P, _P], _I),
+    "ticc_debug_set_step_poll_limit": ([_LL], _I),
     "ticc_ldmd_workspace_size": ([_I, _I, _I, _I, _I, _PSZ], _I),
     "ticc_ldmd_propagate": ([_P, _I, _P, _I, _D, _P, _P, _LL, _P, _LL, _P, _LL, _I, _I, _I, _P, _SZ, _P, _P], _I),
+    "ticc_ldmd_reduced_blocks": ([_P, _SZ, _I, _I, _I, _I, _I, _I, _P, _P], _I),
     "ticc_ldmd_blocks_workspace_size": ([_I, _I, _I, _I, _I, _I, _PSZ], _I),
     "ticc_ldmd_propagate_blocks": ([_P, _I, _P, _I, _D, _P, _P, _LL, _P, _LL, _P, _LL, _LL, _I, _I, _I, _I, _P, _SZ, _P, _P], _I),
     "ticc_contract": ([_P, _P, ctypes.POINTER(_I), _I, _P, _I, _D, _P, _LL, _I, _I, _P, _P, _P, _D, _P, _P], _I),

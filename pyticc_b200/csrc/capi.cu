@@ -233,6 +233,20 @@ int ticc_ldmd_propagate(void* Y, int is_complex, const double* energies, int n_e
                   W_end_stride, 0, n_sector, n_channel, 1, precision, workspace, workspace_bytes, device_status, stream);
 }
 
+int ticc_ldmd_reduced_blocks(const void* workspace, size_t workspace_bytes, int n_channel, int n_energy, int n_block, int n_sector, int is_complex, int precision,
+                             int* counts, void* stream) {
+  if (workspace == nullptr || counts == nullptr) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_ldmd_reduced_blocks: null pointer");
+  const int rc = ldmd_check_sizes("ticc_ldmd_reduced_blocks", n_channel, n_energy, n_block, n_sector, precision);
+  if (rc != TICC_OK) return rc;
+  if (precision != TICC_PRECISION_MIXED) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_ldmd_reduced_blocks: only mixed-precision calls reduce sweep blocks");
+  ticc::LdmdLayout L{};
+  const size_t need = ldmd_layout(L, n_channel, n_energy, n_block, n_sector, is_complex, precision, nullptr);
+  if (workspace_bytes < need) return fail(TICC_ERR_WORKSPACE, "ticc_ldmd_reduced_blocks: workspace of %zu bytes given, %zu needed", workspace_bytes, need);
+  ldmd_layout(L, n_channel, n_energy, n_block, n_sector, is_complex, precision, static_cast<char*>(const_cast<void*>(workspace)));
+  const cudaError_t e = cudaMemcpyAsync(counts, L.reduced, sizeof(int) * (size_t)n_sector, cudaMemcpyDeviceToHost, as_stream(stream));
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_ldmd_reduced_blocks");
+}
+
 int ticc_ldmd_blocks_workspace_size(int n_channel, int n_energy, int n_block, int n_sector, int is_complex, int precision, size_t* bytes) {
   if (bytes == nullptr) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_ldmd_blocks_workspace_size: null output pointer");
   const int rc = ldmd_check_sizes("ticc_ldmd_blocks_workspace_size", n_channel, n_energy, n_block, n_sector, precision);
@@ -457,13 +471,19 @@ int ticc_mlp_adam(float* params, const float* grads, float* moments, int step, f
   return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_mlp_adam");
 }
 
+// ---- test hook: bounded waits ------------------------------------------------------------------
+int ticc_debug_set_step_poll_limit(long long polls) {
+  if (polls < 0) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_debug_set_step_poll_limit: polls=%lld must be non-negative", polls);
+  cudaError_t e = cudaMemcpyToSymbol(ticc::g_step_poll_limit, &polls, sizeof(polls));
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_debug_set_step_poll_limit");
+}
+
 // ---- allocation-free symmetric inversion -------------------------------------------------
-// For callers that cannot allocate device memory themselves: code that runs while a CUDA
-// stream is being captured into a graph (cudaMalloc is not allowed there), plugin hosts
-// that hand this library only the buffers they already own, and drivers written in
-// languages without a device allocator of their own (a Fortran or C program that links
-// just this ABI).  The scratch lives in a fixed array compiled into the library instead
-// of a caller workspace.
+// For callers that cannot allocate device memory themselves: plugin hosts that hand this
+// library only the buffers they already own, runtimes that fix their device memory budget
+// at start-up, and drivers written in languages without a device allocator of their own (a
+// Fortran or C program that links just this ABI).  The scratch lives in a fixed array
+// compiled into the library instead of a caller workspace.
 
 }  // extern "C"
 
@@ -508,9 +528,11 @@ int ticc_sym_inverse_noalloc(void* M, int n, int batch, int is_complex, int* dev
     }
     base = g_noalloc_address[device];
   }
-  // every scratch region is written before it is read (the load kernel fills the whole
-  // padded work matrix, the sweep writes its panels before using them), so nothing needs
-  // clearing between calls
+  // the array keeps the previous call's contents: the work matrix and the panel regions are
+  // fully written before they are read (the load kernel fills the whole padded matrix, the
+  // sweep writes each panel before using it), and the words that must start at zero (the
+  // fused step's work queues, abort flag and row-panel tile flags) are zeroed by
+  // sweep_batched on every call
   sym_layout(n, batch, is_complex, &Mw, &scratch, reinterpret_cast<char*>(base));
   const int np = ticc::ldmd_np(n, is_complex);
   const long long nl = is_complex ? np / 2 : np;

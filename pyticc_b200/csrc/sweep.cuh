@@ -652,17 +652,22 @@ __device__ __forceinline__ int load_acquire(const int* p) {
 }
 __device__ __forceinline__ void store_release(int* p, int v) { asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory"); }
 
+// Polls a wait may spend before it gives up (kStepSpinLimit unless a test lowers it through
+// ticc_debug_set_step_poll_limit; 0 makes every wait give up before its first poll).
+__device__ long long g_step_poll_limit = kStepSpinLimit;
+
 // Thread 0 waits until both flags reach `target`; the CTA learns the outcome.
 __device__ inline bool step_wait(const int* f0, const int* f1, int target, int* abort_flag, int* status, int b, int* slot) {
   if (threadIdx.x == 0) {
     int ok = 1;
+    const long long limit = g_step_poll_limit;
     for (long long it = 0;; ++it) {
-      if (load_acquire(f0) >= target && load_acquire(f1) >= target) break;
-      if (load_acquire(abort_flag) != 0 || it >= kStepSpinLimit) {
+      if (it >= limit || load_acquire(abort_flag) != 0) {
         if (atomicExch(abort_flag, 1) == 0) report_status(status, kDeviceStalled, b, target);
         ok = 0;
         break;
       }
+      if (load_acquire(f0) >= target && load_acquire(f1) >= target) break;
       __nanosleep(128);
     }
     *slot = ok;

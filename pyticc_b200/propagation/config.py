@@ -49,7 +49,10 @@ class Propagation:
     precision: 'fp64' (plain) or 'mixed' (closed channels swept in FP32);
     steps: 'fixed' (the PotentialGrid's sectors) or 'learned' (aligned merges of them
     proposed by ``proposer``, a StepProposer or a path to its weights; None = the
-    packaged default)."""
+    packaged default), used only once a fixed-step solve at the lowest and highest energy
+    of the call agrees with it within ``judge_tol`` (max|dS|, equal open counts);
+    audit: also solve every energy in plain FP64 with fixed steps and attach max|dS| per
+    energy to the result (doubles the cost; for validation runs)."""
 
     mode: PropagationMode = "inelastic"
     memory_mb: float = 512.0
@@ -58,6 +61,8 @@ class Propagation:
     precision: str = "fp64"
     steps: str = "fixed"
     proposer: object = None
+    judge_tol: float = 1.0e-6
+    audit: bool = False
 
     def __post_init__(self) -> None:
         object.__setattr__(self, "device", normalize_device_spec(self.device))
@@ -79,5 +84,13 @@ class Propagation:
             raise ValueError(message)
         if self.steps not in ("fixed", "learned"):
             message = f"Propagation steps must be 'fixed' or 'learned', but got {self.steps!r}"
+            logger.error(message)
+            raise ValueError(message)
+        if not (np.isfinite(self.judge_tol) and self.judge_tol > 0.0):
+            message = f"Propagation judge_tol must be positive, but got {self.judge_tol}"
+            logger.error(message)
+            raise ValueError(message)
+        if not isinstance(self.audit, bool):
+            message = f"Propagation audit must be a boolean, but got {self.audit!r}"
             logger.error(message)
             raise ValueError(message)

@@ -351,6 +351,42 @@ def learned_sectors(hamiltonian, sectors: Sequence[RadialSector], Etot, proposer
     return merged
 
 
+def judged_learned_sectors(problem, potential_grid, Etot, propagation: Propagation) -> tuple[tuple[RadialSector, ...], dict]:
+    """The learned schedule for these energies if the fixed step accepts it, else the fixed
+    grid.  The judge solves the lowest and the highest energy of the call with both
+    schedules (same precision and mode) and accepts when the open counts are equal and
+    max|dS| <= ``propagation.judge_tol``.  Verdicts are cached per schedule on the
+    Hamiltonian, so repeated calls with the same schedule are judged once; a schedule equal
+    to the fixed grid needs no judge.  Returns (sectors, record) with record holding the
+    decision, max|dS| of the judge and both sector counts."""
+    from ..scattering import hamiltonian_for, solve
+
+    hamiltonian = hamiltonian_for(problem, potential_grid)
+    fixed = tuple(potential_grid.sectors)
+    energies = np.atleast_1d(np.asarray(Etot, dtype=np.float64))
+    schedule = learned_sectors(hamiltonian, fixed, energies, resolve_proposer(propagation.proposer), propagation.device)
+    record = {"n_fixed": len(fixed), "n_learned": len(schedule), "accepted": True, "max_dS": 0.0, "judged": False}
+    if len(schedule) == len(fixed):
+        return fixed, record
+    key = ("learned_judge", propagation.precision, propagation.mode, propagation.judge_tol, tuple((s.radial_start, s.radial_end) for s in schedule))
+    cache = getattr(hamiltonian, "_runner_cache", {})
+    verdict = cache.get(key)
+    if verdict is None:
+        probe = np.unique([energies.min(), energies.max()])
+        plain = replace(propagation, steps="fixed", audit=False)
+        a = solve(problem, probe, potential_grid, plain, sectors=fixed)
+        b = solve(problem, probe, potential_grid, plain, sectors=schedule)
+        same_counts = all(x.shape == y.shape for x, y in zip(a.Smat, b.Smat, strict=True))
+        dS = max((float(np.abs(x - y).max()) for x, y in zip(a.Smat, b.Smat, strict=True) if x.size and x.shape == y.shape), default=0.0)
+        verdict = (bool(same_counts and dS <= propagation.judge_tol), dS)
+        cache[key] = verdict
+        if not verdict[0]:
+            logger.warning(f"Learned schedule rejected by the fixed-step judge: max|dS|={dS:.3e}, open counts equal={same_counts}; using the fixed grid")
+        record["judged"] = True
+    record["accepted"], record["max_dS"] = verdict
+    return (schedule if verdict[0] else fixed), record
+
+
 def validate_learned(problem, Etot, potential_grid, propagation: Propagation, proposer: StepProposer, *, tol: float = 1e-6):
     """Solve with the fixed grid and with the learned schedule; return (accepted, max|dS|,
     n_fixed, n_learned, result) where result is the learned solve when accepted and the

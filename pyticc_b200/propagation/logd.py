@@ -10,6 +10,8 @@ CUDA device once.
 
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import torch
 from loguru import logger
@@ -59,10 +61,13 @@ def _is_complex(*values) -> bool:
     return False
 
 
-def propagate_device(Y: torch.Tensor, energies: torch.Tensor, reduced_mass: float, half_steps: torch.Tensor, W_start: torch.Tensor, W_mid: torch.Tensor, W_end: torch.Tensor, *, stride=None, precision: int = nat.PRECISION_FP64) -> torch.Tensor:
+def propagate_device(Y: torch.Tensor, energies: torch.Tensor, reduced_mass: float, half_steps: torch.Tensor, W_start: torch.Tensor, W_mid: torch.Tensor, W_end: torch.Tensor, *, stride=None, precision: int = nat.PRECISION_FP64, reduced_out: list | None = None) -> torch.Tensor:
     """Propagate device-resident Y (complex128 or float64, contiguous) in place through
     the sectors of one call.  ``stride`` overrides the element stride between consecutive
-    sectors of the three W views (e.g. an interleaved point list)."""
+    sectors of the three W views (e.g. an interleaved point list).  In mixed precision,
+    ``reduced_out`` (a list) receives a pinned host int32 tensor that the stream fills with
+    the per-sector counts of 128-wide sweep blocks that took the TF32x3 product (read it
+    after synchronising)."""
     lib = nat.load_library()
     n_energy, n, _ = Y.shape
     n_sector = half_steps.numel()
@@ -82,6 +87,10 @@ def propagate_device(Y: torch.Tensor, energies: torch.Tensor, reduced_mass: floa
             "ticc_ldmd_propagate",
         )
         status.raise_if_failed("ticc_ldmd_propagate")
+        if reduced_out is not None and precision == nat.PRECISION_MIXED:
+            counts = torch.empty(n_sector, dtype=torch.int32, pin_memory=True)
+            nat.check(lib.ticc_ldmd_reduced_blocks(nat.ptr(work), work.numel(), n, n_energy, 1, n_sector, is_complex, precision, ctypes.c_void_p(counts.data_ptr()), nat.stream_handle(dev)), "ticc_ldmd_reduced_blocks")
+            reduced_out.append(counts)
     return Y
 
 

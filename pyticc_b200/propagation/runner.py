@@ -72,16 +72,39 @@ class DeviceHamiltonian:
         return contract_rows(self.rows, potential, radial_points=R, U=self.U, E_int=self.E_int, reduced_mass=self.reduced_mass, out=out)
 
 
-_DEVICE_HAMILTONIANS: dict[tuple[int, int, bool], DeviceHamiltonian] = {}
+def _device_state(hamiltonian, key, build):
+    """Device state cached on the Hamiltonian object itself (its ``_runner_cache``), so the
+    state lives exactly as long as the Hamiltonian; objects without that attribute get a
+    fresh build on every call."""
+    cache = getattr(hamiltonian, "_runner_cache", None)
+    if cache is None:
+        return build()
+    state = cache.get(key)
+    if state is None:
+        state = build()
+        cache[key] = state
+    return state
+
+
+def release_device_state(hamiltonian) -> None:
+    """Drop every device-resident copy this Hamiltonian holds (they are rebuilt on use)."""
+    cache = getattr(hamiltonian, "_runner_cache", None)
+    if cache is not None:
+        cache.clear()
 
 
 def device_hamiltonian(hamiltonian, device: torch.device, closed_first: bool = False) -> DeviceHamiltonian:
-    key = (id(hamiltonian), device.index, closed_first)
-    cached = _DEVICE_HAMILTONIANS.get(key)
-    if cached is None:
-        cached = DeviceHamiltonian(hamiltonian, device, closed_first)
-        _DEVICE_HAMILTONIANS[key] = cached
-    return cached
+    return _device_state(hamiltonian, ("exact", device.index, closed_first), lambda: DeviceHamiltonian(hamiltonian, device, closed_first))
+
+
+def finish_stats(stats: dict) -> dict:
+    """Synchronise and fold the pending reduced-block counts of ``propagate(stats=...)``
+    into stats["reduced_steps"] (two sweeps per sector take the same count)."""
+    pending = stats.pop("_reduced", [])
+    if pending:
+        torch.cuda.synchronize()
+    stats["reduced_steps"] = stats.get("reduced_steps", 0) + sum(2 * int(c.sum()) for c in pending)
+    return stats
 
 
 def initial_logD(W0: torch.Tensor, energies: torch.Tensor, reduced_mass: float, mode: str) -> torch.Tensor:
@@ -93,11 +116,14 @@ def initial_logD(W0: torch.Tensor, energies: torch.Tensor, reduced_mass: float, 
     return torch.diag_embed(values).contiguous()
 
 
-def propagate(hamiltonian, Etot, radial_sectors: Sequence[RadialSector], config: Propagation, *, Y_initial: torch.Tensor | None = None, window_timing: list | None = None) -> torch.Tensor:
+def propagate(hamiltonian, Etot, radial_sectors: Sequence[RadialSector], config: Propagation, *, Y_initial: torch.Tensor | None = None, window_timing: list | None = None, stats: dict | None = None) -> torch.Tensor:
     """Y at the last sector end for every energy, on the device (runner.py:112-161).
 
     ``window_timing`` (optional list) receives (start event, stop event, algorithmic
-    flops) per LDMD launch: two symmetric N x N inversions (N^3 each) per (sector, energy)."""
+    flops) per LDMD launch: two symmetric N x N inversions (N^3 each) per (sector, energy).
+    ``stats`` (optional dict) receives the sector count, the sweep steps and, in mixed
+    precision, the device's per-sector reduced-block counts as pending host copies;
+    ``finish_stats`` turns them into "reduced_steps" (no synchronisation until then)."""
     energies_np = get_Etot(Etot)
     dev = resolve_device(config.device)
     if not radial_sectors:
@@ -133,10 +159,15 @@ def propagate(hamiltonian, Etot, radial_sectors: Sequence[RadialSector], config:
         if window_timing is not None:
             t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             t0.record()
-        propagate_device(Y, energies, dh.reduced_mass, halves, Wv[0::2], Wv[1::2], Wv[2::2], stride=(stride, stride, stride), precision=precision)
+        reduced = stats.setdefault("_reduced", []) if stats is not None and mixed else None
+        propagate_device(Y, energies, dh.reduced_mass, halves, Wv[0::2], Wv[1::2], Wv[2::2], stride=(stride, stride, stride), precision=precision, reduced_out=reduced)
         if window_timing is not None:
             t1.record()
             window_timing.append((t0, t1, 2.0 * float(n) ** 3 * len(window) * energies.numel()))
+        if stats is not None:
+            blocks = -(-(2 * n if config.mode == "capture" else n) // 128)
+            stats["sectors"] = stats.get("sectors", 0) + len(window)
+            stats["sweep_steps"] = stats.get("sweep_steps", 0) + 2 * blocks * len(window)
         done += len(window)
         if config.print_verbose and (done == n_sector or done >= next_report):
             torch.cuda.synchronize(dev)
@@ -210,16 +241,8 @@ class DeviceBlocks:
         return self._contract(self.rows[g], radial_points, self.U[g], E_int, out=out)
 
 
-_DEVICE_BLOCKS: dict = {}
-
-
 def device_blocks(hamiltonian, blocks, device: torch.device, closed_first: bool = False) -> DeviceBlocks:
-    key = (id(hamiltonian), blocks, device.index, closed_first)
-    cached = _DEVICE_BLOCKS.get(key)
-    if cached is None:
-        cached = DeviceBlocks(hamiltonian, blocks, device, closed_first)
-        _DEVICE_BLOCKS[key] = cached
-    return cached
+    return _device_state(hamiltonian, ("blocks", blocks, device.index, closed_first), lambda: DeviceBlocks(hamiltonian, blocks, device, closed_first))
 
 
 def blocks_window(n_channel: int, n_block: int, n_sector: int) -> int:

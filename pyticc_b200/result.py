@@ -35,10 +35,22 @@ class ScatteringResult:
     L: np.ndarray
     Smat: tuple[np.ndarray, ...]
     timing: Timing | None = None
+    reduced_mass: float | None = None
+    # filled by an audited solve (Propagation(audit=True)): per energy, max|S - S_fp64| against
+    # an all-FP64 fixed-step solve of the same block on the same device
+    max_dS: np.ndarray | None = None
 
     @property
     def Y_asymptotic(self) -> np.ndarray:
         return _transform_logD(self.Y_propagated, self.asymptotic_transform)
+
+    def partial_cross_sections(self):
+        """Level-to-level cross sections of this (J, parity) block (bohr^2)."""
+        from .cross_section import partial_cross_sections
+
+        if self.reduced_mass is None:
+            raise ValueError("partial cross sections need the reduced mass of the solve")
+        return partial_cross_sections(self.basis, self.Etot, self.Smat, self.reduced_mass)
 
     @property
     def open_channel_indices(self) -> tuple[np.ndarray, ...]:

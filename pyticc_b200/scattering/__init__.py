@@ -7,6 +7,7 @@ channel and row construction are host setup; propagation and matching run on the
 
 from __future__ import annotations
 
+from collections import OrderedDict
 from collections.abc import Sequence
 from dataclasses import dataclass, field, replace
 from time import perf_counter, process_time
@@ -153,6 +154,9 @@ class ScattHamiltonian:
     approx: Approx = Approx.EXACT
     K_delta: int = 1
     _device_cache: DeviceBasisCache = field(default_factory=DeviceBasisCache, compare=False, repr=False)
+    # device-resident propagation state (rows, U, E_int, channel order) per device and
+    # channel selection; it lives and dies with this Hamiltonian
+    _runner_cache: dict = field(default_factory=dict, compare=False, repr=False)
 
     def __post_init__(self) -> None:
         if self.K_delta < 1:
@@ -206,17 +210,28 @@ def build_hamiltonian(system: ScattSystem, potential_grid: PotentialGrid) -> Sca
     return ScattHamiltonian(system.basis, float(system.reduced_mass), vb, potential_grid, system.approx, system.K_delta)
 
 
-_HAMILTONIANS: dict[tuple[int, int], ScattHamiltonian] = {}
+HAMILTONIAN_CACHE_SIZE = 8
+_HAMILTONIANS: OrderedDict[tuple[int, int], tuple[ScattSystem, PotentialGrid, ScattHamiltonian]] = OrderedDict()
 
 
 def hamiltonian_for(system: ScattSystem, potential_grid: PotentialGrid) -> ScattHamiltonian:
-    """Build once per (system, grid) pair and reuse (the rows only depend on geometry)."""
+    """Build once per (system, grid) pair and reuse (the rows only depend on geometry).
+
+    The cache holds the system and grid it was built from and checks their identity, so an
+    object id reused after garbage collection can never be served another system's
+    Hamiltonian; it keeps the most recent HAMILTONIAN_CACHE_SIZE pairs, and an evicted
+    Hamiltonian frees its device state with it."""
     key = (id(system), id(potential_grid))
-    cached = _HAMILTONIANS.get(key)
-    if cached is None or cached.basis is not system.basis or cached.potential_grid is not potential_grid:
-        cached = build_hamiltonian(system, potential_grid)
-        _HAMILTONIANS[key] = cached
-    return cached
+    entry = _HAMILTONIANS.get(key)
+    if entry is not None and entry[0] is system and entry[1] is potential_grid:
+        _HAMILTONIANS.move_to_end(key)
+        return entry[2]
+    hamiltonian = build_hamiltonian(system, potential_grid)
+    _HAMILTONIANS[key] = (system, potential_grid, hamiltonian)
+    _HAMILTONIANS.move_to_end(key)
+    while len(_HAMILTONIANS) > HAMILTONIAN_CACHE_SIZE:
+        _HAMILTONIANS.popitem(last=False)
+    return hamiltonian
 
 
 def build_k_blocks(hamiltonian: ScattHamiltonian) -> tuple[KBlock, ...]:
@@ -249,13 +264,15 @@ def finalize_K_block(basis, block: KBlock, Y_BF: torch.Tensor, Etot, reduced_mas
     return KBlockResult(block, open_indices, Y_BF.cpu().numpy(), B, L, smats)
 
 
-def solve(problem: ScattSystem, Etot, potential_grid: PotentialGrid, propagation: Propagation, *, sectors: Sequence[RadialSector] | None = None) -> ScatteringResult | CoupledStatesResult:
+def solve(problem: ScattSystem, Etot, potential_grid: PotentialGrid, propagation: Propagation, *, sectors: Sequence[RadialSector] | None = None, stats: dict | None = None) -> ScatteringResult | CoupledStatesResult:
     """Build (or reuse), propagate and match one (J, parity) system (reference
     solver.py:57-178): exact CC returns a ScatteringResult; CS and NNCC propagate their K
     blocks together and return a CoupledStatesResult.
 
     ``sectors`` optionally replaces the grid's fixed-step sectors by another schedule whose
-    start/mid/end points all lie on the grid (e.g. a learned step schedule)."""
+    start/mid/end points all lie on the grid (e.g. a learned step schedule).  ``stats``
+    (optional dict, exact CC) receives the sectors propagated, the reduced-precision sweep
+    steps among all sweep steps, and the learned-schedule judge's record."""
     from ..propagation.runner import propagate, propagate_blocks
 
     if not isinstance(problem, ScattSystem):
@@ -292,12 +309,22 @@ def solve(problem: ScattSystem, Etot, potential_grid: PotentialGrid, propagation
         logger.info(f"Solver complete: {timing}")
         return CoupledStatesResult(basis, energies, problem.approx, results, timing)
     if sectors is None and propagation.steps == "learned":
-        from ..propagation.learned import learned_sectors, resolve_proposer
+        from ..propagation.learned import judged_learned_sectors
 
-        run_sectors = learned_sectors(hamiltonian, run_sectors, energies, resolve_proposer(propagation.proposer), propagation.device)
-    Y = propagate(hamiltonian, energies, run_sectors, propagation)
+        run_sectors, record = judged_learned_sectors(problem, potential_grid, energies, propagation)
+        if stats is not None:
+            stats["learned"] = record
+    Y = propagate(hamiltonian, energies, run_sectors, propagation, stats=stats)
     B, L = get_Bmat_BF_to_SF(basis)
     smats = _match(Y, B, L, basis.E_int, run_sectors[-1].radial_end, energies, hamiltonian.reduced_mass)
+    max_dS = None
+    if propagation.audit:
+        plain = solve(problem, energies, potential_grid, replace(propagation, precision="fp64", steps="fixed", audit=False))
+        max_dS = np.asarray([float(np.abs(a - b).max()) if a.shape == b.shape and a.size else (0.0 if a.shape == b.shape else np.inf) for a, b in zip(smats, plain.Smat, strict=True)])
+    if stats is not None:
+        from ..propagation.runner import finish_stats
+
+        finish_stats(stats)
     timing = Timing(perf_counter() - wall, process_time() - cpu)
     logger.info(f"Solver complete: {timing}")
-    return ScatteringResult(basis, energies, Y.cpu().numpy(), B, L, smats, timing)
+    return ScatteringResult(basis, energies, Y.cpu().numpy(), B, L, smats, timing, hamiltonian.reduced_mass, max_dS)

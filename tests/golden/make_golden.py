@@ -538,6 +538,147 @@ def make_solve_kblocks() -> None:
     )
 
 
+# ----------------------------------------------------------------------------------------
+# Benchmark-size fixtures (minutes of CPU each; only S, open counts and energies are kept)
+# ----------------------------------------------------------------------------------------
+BENCH_ENERGIES_CM = np.linspace(100.0, 3000.0, 256)  # the vibrating A+BC energy grid
+
+
+def _solve_full_and_save(name, params, system, boundaries, halves, energies, mode, **quad):
+    import time
+
+    grid = ticc.prepare_potential(system, boundaries, halves, **quad)
+    started = time.perf_counter()
+    result = ticc.solve(system, energies, grid, ticc.Propagation(mode=mode, memory_mb=2048.0, device="cpu"))
+    params = {**params, "reference_wall_s": time.perf_counter() - started, "n_channel": int(system.basis.n_channel), "n_sector": len(grid.sectors)}
+    n_open = np.asarray([m.shape[0] for m in result.Smat])
+    width = int(max(n_open.max(), 1))
+    _save(name, params, energies=np.asarray(energies), n_open=n_open, Smat=_pad_smat(result.Smat, width), E_int=system.basis.E_int)
+
+
+def make_full_rigid() -> None:
+    """The CPU-runnable rigid-rotor configuration at full size: N=231, 275 sectors, 16 energies."""
+    params = {"B_cm": 20.0, "jmax": 20, "J": 20, "parity": 1, "mu_amu": 18.0, "eps_cm": 150.0, "Rm": 6.5, "a1": 0.3, "a2": 0.2, "n_theta": 24, "boundaries": [2.5, 30.0], "half_steps": [0.05]}
+    system = ticc.build_ScattSystem(
+        ticc.AtomSpec(),
+        _rigid_rotor(params["B_cm"], params["jmax"]),
+        Jtot=params["J"],
+        system_parity=1,
+        potential=_lj_aniso_pes(params["eps_cm"], params["Rm"], params["a1"], params["a2"]),
+        reduced_mass=params["mu_amu"] * AMU,
+    )
+    energies = np.linspace(10.0, 500.0, 16) * CM
+    _solve_full_and_save("full_rigid_J20", params, system, params["boundaries"], params["half_steps"], energies, "inelastic", n_theta=params["n_theta"])
+
+
+def make_full_morse() -> None:
+    """The vibrating A+BC benchmark blocks at full size (N=1984 / 1860, 938 sectors) at two of
+    the benchmark energies, one low and one near the top of the grid."""
+    params = {
+        "De_cm": 40000.0, "re": 1.4, "a": 1.2, "diatom_mass_amu": 1.0, "r_interval": [0.5, 3.5], "n_dvr": 32, "vmax": 3, "jmax": 30, "J": 30,
+        "mu_amu": 18.0, "eps_cm": 150.0, "Rm": 6.5, "a1": 0.3, "a2": 0.2, "seed": 2024, "n_theta": 32, "boundaries": [2.5, 40.0], "half_steps": [0.02],
+        "energy_indices": [0, 250],
+    }
+    c1, c2 = np.random.default_rng(params["seed"]).uniform(-0.5, 0.5, size=2)
+    params["c1"], params["c2"] = float(c1), float(c2)
+    mass = params["diatom_mass_amu"] * AMU
+
+    def morse(r):
+        return params["De_cm"] * CM * (1.0 - np.exp(-params["a"] * (r - params["re"]))) ** 2
+
+    dvr = build_SineDVR(params["r_interval"][0], params["r_interval"][1], params["n_dvr"], mass, morse)
+    rovib = build_RovibDVR(dvr, params["vmax"], params["jmax"], mass)
+    diatom = ticc.DiatomBasis(rovib=rovib, energy_zero=float(rovib.E_vj[0, 0]))
+    energies = BENCH_ENERGIES_CM[params["energy_indices"]] * CM
+    parities = [int(p) for p in sys.argv[3:]] if len(sys.argv) > 3 and sys.argv[2] == "full_morse" else [1, -1]
+    for parity in parities:
+        system = ticc.build_ScattSystem(
+            ticc.AtomSpec(),
+            diatom,
+            Jtot=params["J"],
+            system_parity=parity,
+            potential=_lj_aniso_pes(params["eps_cm"], params["Rm"], params["a1"], params["a2"], c1, c2, params["re"]),
+            reduced_mass=params["mu_amu"] * AMU,
+        )
+        tag = "+" if parity > 0 else "-"
+        _solve_full_and_save(f"full_morse_J30_p{tag}", {**params, "parity": parity}, system, params["boundaries"], params["half_steps"], energies, "inelastic", n_theta=params["n_theta"])
+
+
+def make_full_capture() -> None:
+    """The ultracold capture block at full size: rigid rotor B=0.03 cm^-1, j<=40, J=10 (N=396),
+    capture boundary at 8 bohr, fixed step h=0.05 to 1500 bohr, at 1 uK and 1 mK."""
+    params = {"B_cm": 0.03, "jmax": 40, "J": 10, "parity": 1, "mu_amu": 100.0, "C6": 1.0e4, "wall_cm": 500.0, "seed": 3, "n_theta": 48, "boundaries": [8.0, 1500.0], "half_steps": [0.05], "energies_K": [1.0e-6, 1.0e-3]}
+    g = np.random.default_rng(params["seed"]).uniform(0.2, 1.0, size=3)
+
+    def interaction(R, coordinates):
+        _, theta = coordinates
+        x = np.cos(theta)
+        p2 = 0.5 * (3.0 * x * x - 1.0)
+        wall = params["wall_cm"] * CM * np.exp(-(((R - 7.0) / 1.5) ** 2)) * (g[0] + g[1] * x + g[2] * p2)
+        return -params["C6"] / R**6 * (1.0 + 0.1 * p2) + wall
+
+    system = ticc.build_ScattSystem(
+        ticc.AtomSpec(),
+        _rigid_rotor(params["B_cm"], params["jmax"]),
+        Jtot=params["J"],
+        system_parity=params["parity"],
+        potential=ticc.PESWrapper(interaction=interaction),
+        reduced_mass=params["mu_amu"] * AMU,
+    )
+    energies = np.asarray(params["energies_K"]) * K2AU
+    _solve_full_and_save("full_capture_J10", params, system, params["boundaries"], params["half_steps"], energies, "capture", n_theta=params["n_theta"])
+
+
+def make_dropin() -> None:
+    """Every call the reference's own runner makes to ``propagate_logD`` (runner.py:293) during
+    a solve split into several radial windows: arguments and result, for a replay through the
+    CUDA ``propagate_logD``, plus the solve's S matrices."""
+    import pyticc.propagation.runner as ref_runner
+
+    params = {"B_cm": 20.0, "jmax": 7, "J": 5, "parity": 1, "mu_amu": 18.0, "eps_cm": 150.0, "Rm": 6.5, "a1": 0.3, "a2": 0.2, "n_theta": 10, "boundaries": [2.5, 5.0, 9.0], "half_steps": [0.04, 0.08], "memory_mb": 3.0}
+    system = ticc.build_ScattSystem(
+        ticc.AtomSpec(),
+        _rigid_rotor(params["B_cm"], params["jmax"]),
+        Jtot=params["J"],
+        system_parity=params["parity"],
+        potential=_lj_aniso_pes(params["eps_cm"], params["Rm"], params["a1"], params["a2"]),
+        reduced_mass=params["mu_amu"] * AMU,
+    )
+    energies = np.array([20.0, 260.0, 480.0]) * CM
+    grid = ticc.prepare_potential(system, params["boundaries"], params["half_steps"], n_theta=params["n_theta"])
+    calls = []
+    original = ref_runner.propagate_logD
+
+    def recording(Y_initial, total_energies, reduced_mass, radial_half_steps, W_base_start, W_base_mid, W_base_end, **kwargs):
+        out = original(Y_initial, total_energies, reduced_mass, radial_half_steps, W_base_start, W_base_mid, W_base_end, **kwargs)
+        calls.append({k: np.asarray(v) for k, v in (("Y_initial", Y_initial), ("total_energies", total_energies), ("radial_half_steps", radial_half_steps), ("W_base_start", W_base_start), ("W_base_mid", W_base_mid), ("W_base_end", W_base_end), ("Y_final", out))} | {"reduced_mass": np.asarray(reduced_mass)})
+        return out
+
+    ref_runner.propagate_logD = recording
+    try:
+        result = ticc.solve(system, energies, grid, ticc.Propagation(mode="inelastic", memory_mb=params["memory_mb"], device="cpu"))
+    finally:
+        ref_runner.propagate_logD = original
+    import inspect
+
+    arrays = {f"call{i}_{k}": v for i, c in enumerate(calls) for k, v in c.items()}
+    params["n_calls"] = len(calls)
+    params["signature"] = str(inspect.signature(original))
+    params["parameters"] = [[name, str(parameter.kind)] for name, parameter in inspect.signature(original).parameters.items()]
+    _save(
+        "dropin_calls",
+        params,
+        energies=energies,
+        E_int=system.basis.E_int,
+        Bmat=result.asymptotic_transform,
+        L=result.L,
+        Rmatch=np.asarray(grid.sectors[-1].radial_end),
+        Smat=_pad_smat(result.Smat, system.basis.n_channel),
+        n_open=np.asarray([m.shape[0] for m in result.Smat]),
+        **arrays,
+    )
+
+
 MAKERS = {
     "ldmd": make_ldmd,
     "contract": make_contract,
@@ -550,9 +691,20 @@ MAKERS = {
     "channel_counts": make_channel_counts,
     "kblocks": make_kblocks,
     "solve_kblocks": make_solve_kblocks,
+    "dropin": make_dropin,
+}
+# benchmark-size fixtures: run by name only (tens of minutes of CPU in total);
+# ``full_morse`` takes optional parities after its name: ``make_golden.py <src> full_morse -1``
+FULL_SIZE_MAKERS = {
+    "full_rigid": make_full_rigid,
+    "full_morse": make_full_morse,
+    "full_capture": make_full_capture,
 }
 
 if __name__ == "__main__":
-    # python make_golden.py <reference src> [fixture names...]  (default: all)
-    for key in sys.argv[2:] or list(MAKERS):
-        MAKERS[key]()
+    # python make_golden.py <reference src> [fixture names...]  (default: all small fixtures)
+    names = sys.argv[2:] or list(MAKERS)
+    if names and names[0] == "full_morse":
+        names = ["full_morse"]
+    for key in names:
+        {**MAKERS, **FULL_SIZE_MAKERS}[key]()

@@ -263,14 +263,82 @@ def test_mixed_precision_matches_fp64_on_vibrating_block():
     assert mixed.unitarity_defect().max() < 1e-6
 
 
-@pytest.mark.parametrize("name", ["solve_rigid_p+", "solve_morse"])
-def test_mixed_precision_matches_reference(name):
-    g, p, wl = _golden_workload(name)
-    result = tb.solve(wl.system, wl.energies, wl.grid, tb.Propagation(precision="mixed"))
-    for e, s in enumerate(result.Smat):
-        n = s.shape[0]
-        if n:
-            assert np.abs(s - g["Smat"][e, :n, :n]).max() <= MIXED_TOL
+def test_mixed_precision_matches_oracle_where_reduced_steps_run():
+    """A vibrating block of more than 256 channels over a short inner grid (2.5-4.5 bohr,
+    inside the repulsive wall, where every leading block is strongly closed): the mixed
+    solve takes TF32x3 steps (counted through ticc_ldmd_reduced_blocks) and still matches
+    the oracle's all-FP64 LAPACK propagation and matching within 1e-6."""
+    wl = workloads.morse_atom_diatom(J=8, jmax=12, vmax=3, n_dvr=24, n_theta=16, boundaries=(2.5, 4.5), half_steps=(0.02,), energies_cm=[150.0, 2900.0])
+    assert wl.system.basis.n_channel > 256
+    stats: dict = {}
+    mixed = tb.solve(wl.system, wl.energies, wl.grid, tb.Propagation(precision="mixed"), stats=stats)
+    assert stats["reduced_steps"] >= stats["sweep_steps"] // 2, stats
+    vb = tb.scattering.hamiltonian_for(wl.system, wl.grid).V_basis
+    _, S = o_pipeline.solve(
+        wl.system.basis.E_int, tb.get_Umat_BF(wl.system.basis), vb.channel_indices, vb.B_real, None, 1.0,
+        wl.grid.values.reshape(wl.grid.radial_points.size, -1), wl.grid.radial_points,
+        np.asarray([s.radial_half_step for s in wl.grid.sectors]), wl.system.reduced_mass, wl.energies, mixed.asymptotic_transform, mixed.L,
+    )
+    for a, b in zip(mixed.Smat, S, strict=True):
+        assert a.shape == b.shape
+        if a.size:
+            assert np.abs(a - b).max() <= MIXED_TOL
+
+
+def test_fused_step_wait_gives_up_reports_status_and_the_context_survives():
+    """With the poll limit at 0 every wait of the fused sweep step gives up at once: the
+    call reports device status 6 instead of hanging, and the next call (default limit)
+    computes the right inverse on the same context."""
+    lib = nat.load_library()
+    rng = np.random.default_rng(6)
+    A = rng.normal(size=(4, 300, 300))
+    A = A + A.transpose(0, 2, 1) + np.diag(rng.uniform(3.0, 6.0, 300)) * np.sqrt(300)
+    nat.check(lib.ticc_debug_set_step_poll_limit(0), "ticc_debug_set_step_poll_limit")
+    try:
+        with pytest.raises(RuntimeError, match="gave up waiting"):
+            _sym_inverse(A, False)
+    finally:
+        nat.check(lib.ticc_debug_set_step_poll_limit(1 << 22), "ticc_debug_set_step_poll_limit")
+    X = _sym_inverse(A, False)
+    inv = np.linalg.inv(A)
+    np.testing.assert_allclose(X, inv, rtol=0, atol=1e-13 * np.abs(inv).max())
+
+
+def test_learned_schedule_is_judged_inside_solve():
+    """solve(steps='learned') runs the fixed-step judge: an accepted schedule is used (fewer
+    sectors, within 1e-6 of the fixed-step S) and its verdict is cached; with a tolerance no
+    schedule can meet, the solve falls back to the fixed grid and equals the fixed-step solve."""
+    from pyticc_b200.propagation.learned import train_proposer, training_set
+    from pyticc_b200.scattering import hamiltonian_for
+
+    wl = workloads.ultracold_capture(jmax=6, J=1, parity=-1, boundaries=(8.0, 300.0), n_energy=6)
+    base = tb.Propagation(mode="capture")
+    X, T = training_set([(hamiltonian_for(wl.system, wl.grid), wl.grid.sectors, wl.energies[[0, 5]], base)], max_level=8)
+    proposer, _ = train_proposer(X, T, steps=2000)
+    energies = wl.energies[[2, 3]]
+    fixed = tb.solve(wl.system, energies, wl.grid, base)
+    stats: dict = {}
+    learned = tb.solve(wl.system, energies, wl.grid, tb.Propagation(mode="capture", steps="learned", proposer=proposer), stats=stats)
+    record = stats["learned"]
+    assert record["accepted"] and record["judged"] and record["n_learned"] < record["n_fixed"]
+    assert max(float(np.abs(a - b).max()) for a, b in zip(fixed.Smat, learned.Smat, strict=True) if a.size) <= MIXED_TOL
+    again: dict = {}
+    tb.solve(wl.system, energies, wl.grid, tb.Propagation(mode="capture", steps="learned", proposer=proposer), stats=again)
+    assert not again["learned"]["judged"]  # the cached verdict
+    strict: dict = {}
+    refused = tb.solve(wl.system, energies, wl.grid, tb.Propagation(mode="capture", steps="learned", proposer=proposer, judge_tol=1e-300), stats=strict)
+    assert not strict["learned"]["accepted"] and strict["sectors"] == record["n_fixed"]
+    for a, b in zip(fixed.Smat, refused.Smat, strict=True):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_audit_attaches_max_dS_against_plain_fp64():
+    wl = workloads.morse_atom_diatom(J=8, jmax=12, vmax=3, n_dvr=24, n_theta=16, boundaries=(2.5, 12.0), half_steps=(0.02,), energies_cm=[150.0, 2900.0])
+    audited = tb.solve(wl.system, wl.energies, wl.grid, tb.Propagation(precision="mixed", audit=True))
+    plain = tb.solve(wl.system, wl.energies, wl.grid, tb.Propagation())
+    want = [float(np.abs(a - b).max()) if a.size else 0.0 for a, b in zip(audited.Smat, plain.Smat, strict=True)]
+    np.testing.assert_array_equal(audited.max_dS, want)
+    assert audited.max_dS.max() <= MIXED_TOL
 
 
 def test_assembled_W_base_is_exactly_symmetric():

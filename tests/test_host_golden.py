@@ -125,3 +125,15 @@ def test_open_blocks_to_host_copies_only_the_open_corner():
     for e, o in enumerate(out):
         np.testing.assert_array_equal(o, S[e, : n_open[e], : n_open[e]].numpy())
     assert [o.shape for o in open_blocks_to_host(S[:1], np.array([0]))] == [(0, 0)]
+
+
+def test_propagate_logD_keeps_the_reference_signature():
+    """The parameter names and kinds of the reference's propagate_logD (recorded from the
+    reference at the runner.py:293 call site) are this library's, so the runner's call binds."""
+    import inspect
+
+    from pyticc_b200.propagation.logd import propagate_logD
+
+    _, params = load_golden("dropin_calls")
+    ours = [[name, str(p.kind)] for name, p in inspect.signature(propagate_logD).parameters.items()]
+    assert ours == params["parameters"]

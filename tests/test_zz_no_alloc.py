@@ -1,7 +1,8 @@
 """The allocation-free inversion entry point against the workspace one.
 
-Some callers cannot allocate device memory (code running under stream capture, plugin
-hosts that pass only their own buffers, C/Fortran drivers without a device allocator);
+Some callers cannot allocate device memory (plugin hosts that pass only their own buffers,
+runtimes that fix their device memory budget at start-up, C/Fortran drivers without a
+device allocator);
 ``ticc_sym_inverse_noalloc`` serves them from a fixed device array inside the library.
 This file is collected last on purpose: it must pass both alone in a fresh process and
 after every other test has used the library.
@@ -53,7 +54,9 @@ def _matrices(seed: int, n: int, batch: int, is_complex: bool) -> np.ndarray:
 
 @pytest.mark.parametrize("is_complex", [False, True])
 def test_no_alloc_inverse_matches_workspace_inverse_on_two_calls(is_complex):
-    for call, (n, batch) in enumerate([(300, 3), (200, 2)]):
+    # 300 and 200: several pivot blocks (fused sweep steps); 100: one pivot block (real) or
+    # two (complex); 40: the 64-wide single-block inversion (real) or one 128 block (complex)
+    for call, (n, batch) in enumerate([(300, 3), (200, 2), (100, 4), (40, 3)]):
         A = _matrices(10 + call, n, batch, is_complex)
         want = _with_workspace(A, is_complex)
         got = _no_alloc(A, is_complex)
