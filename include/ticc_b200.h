@@ -87,6 +87,19 @@ int ticc_sym_inverse_noalloc(void* M, int n, int batch, int is_complex, int* dev
  * and the context stays usable.  Applies to the current device. */
 int ticc_debug_set_step_poll_limit(long long polls);
 
+/* Test hook with no counterpart in the reference: the tcgen05 TF32x3 trailing-update tile
+ * run on its own.  For each listed tile t (tiles[3t .. 3t+2] = matrix b, row tile ta,
+ * column tile tb, device ints) it computes, in the 128 x 128 block (ta, tb) of matrix b of
+ * M (batch x np x np FP64, np a multiple of 128),
+ *     M_tile <- M_tile - cold[b][:, ta block]^T U[b][:, tb block]
+ * with cold and U given as batch x 128 x np FP64 panels (device), split into TF32 hi/lo
+ * words, the three products hi*hi + hi*lo + lo*hi accumulated in FP32 in tensor memory.  A
+ * diagonal tile (ta == tb) keeps its lower half and mirrors it into the upper half.
+ * Listed tiles must be distinct. */
+int ticc_debug_tc_update_workspace_size(int np, int batch, size_t* bytes);
+int ticc_debug_tc_update(double* M, int np, int batch, const double* cold, const double* U, const int* tiles, int n_tiles, void* workspace,
+                         size_t workspace_bytes, int* device_status, void* stream);
+
 /* ---- LDMD propagation -------------------------------------------------------
  * Propagate n_energy log-derivative matrices Y through n_sector Manolopoulos LDMD
  * sectors.  Replaces propagate_logD (propagation/logd.py:340-398) with its

@@ -49,6 +49,8 @@ SIGNATURES: dict[str, tuple[list, type]] = {
     "ticc_sym_inverse": ([_P, _I, _I, _I, _P, _SZ, _P, _P], _I),
     "ticc_sym_inverse_noalloc": ([_P, _I, _I, _I, _P, _P], _I),
     "ticc_debug_set_step_poll_limit": ([_LL], _I),
+    "ticc_debug_tc_update_workspace_size": ([_I, _I, _PSZ], _I),
+    "ticc_debug_tc_update": ([_P, _I, _I, _P, _P, _P, _I, _P, _SZ, _P, _P], _I),
     "ticc_ldmd_workspace_size": ([_I, _I, _I, _I, _I, _PSZ], _I),
     "ticc_ldmd_propagate": ([_P, _I, _P, _I, _D, _P, _P, _LL, _P, _LL, _P, _LL, _I, _I, _I, _P, _SZ, _P, _P], _I),
     "ticc_ldmd_reduced_blocks": ([_P, _SZ, _I, _I, _I, _I, _I, _I, _P, _P], _I),

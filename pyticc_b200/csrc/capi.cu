@@ -15,6 +15,7 @@
 #include "ldmd.cuh"
 #include "match.cuh"
 #include "sweep.cuh"
+#include "tc_update.cuh"
 
 namespace {
 
@@ -65,7 +66,8 @@ size_t ldmd_layout(ticc::LdmdLayout& L, int n, int n_energy, int n_block, int n_
   L.scratch_doubles = need_e > need_s ? need_e : need_s;
   L.scratch = c.take<double>(L.scratch_doubles);
   L.reduced = (precision == TICC_PRECISION_MIXED) ? c.take<int>((size_t)n_sector) : nullptr;
-  if (base == nullptr) L.reduced = nullptr;
+  L.split = (precision == TICC_PRECISION_MIXED) ? c.take<float>(ticc::tc_split_floats(L.np, (int)batch)) : nullptr;
+  if (base == nullptr) L.reduced = nullptr, L.split = nullptr;
   return c.used + 256;
 }
 
@@ -469,6 +471,54 @@ int ticc_mlp_adam(float* params, const float* grads, float* moments, int step, f
   ticc::note_launch();
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_mlp_adam");
+}
+
+// ---- test hook: the tcgen05 TF32x3 update tile on its own -------------------------------------
+static size_t tc_debug_layout(int np, int batch, float** split, int** flag, char* base) {
+  Carver c{base};
+  *split = c.take<float>(ticc::tc_split_floats(np, batch));
+  *flag = c.take<int>(4);
+  return c.used + 256;
+}
+
+int ticc_debug_tc_update_workspace_size(int np, int batch, size_t* bytes) {
+  if (bytes == nullptr || np < ticc::kBlock || np % ticc::kBlock != 0 || batch < 1)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_debug_tc_update_workspace_size: np=%d (a positive multiple of 128) batch=%d", np, batch);
+  float* split;
+  int* flag;
+  *bytes = tc_debug_layout(np, batch, &split, &flag, nullptr);
+  return TICC_OK;
+}
+
+int ticc_debug_tc_update(double* M, int np, int batch, const double* cold, const double* U, const int* tiles, int n_tiles, void* workspace, size_t workspace_bytes,
+                         int* device_status, void* stream) {
+  if (M == nullptr || cold == nullptr || U == nullptr || tiles == nullptr || n_tiles < 0 || np < ticc::kBlock || np % ticc::kBlock != 0 || batch < 1)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_debug_tc_update: bad arguments (np=%d batch=%d n_tiles=%d)", np, batch, n_tiles);
+  float* split;
+  int* flag;
+  const size_t need = tc_debug_layout(np, batch, &split, &flag, nullptr);
+  if (workspace == nullptr || workspace_bytes < need) return fail(TICC_ERR_WORKSPACE, "ticc_debug_tc_update: workspace of %zu bytes given, %zu needed", workspace_bytes, need);
+  tc_debug_layout(np, batch, &split, &flag, static_cast<char*>(workspace));
+  cudaStream_t s = as_stream(stream);
+  cudaError_t e = cudaMemsetAsync(flag, 0, 4 * sizeof(int), s);
+  if (e != cudaSuccess) return cuda_fail(e, "ticc_debug_tc_update: memset");
+  ticc::tc_split_panels_kernel<<<dim3(np / ticc::kBlock, batch), 256, 0, s>>>(cold, U, np, batch, split);
+  ticc::note_launch();
+  if (n_tiles == 0) return TICC_OK;
+  ticc::TcMaps maps;
+  e = ticc::tc_make_maps(maps, split, M, np, (long long)np * np, batch);
+  if (e != cudaSuccess) return cuda_fail(e, "ticc_debug_tc_update: tensor maps");
+  e = cudaFuncSetAttribute(ticc::tc_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, ticc::kTcSmemBytes);
+  if (e != cudaSuccess) return cuda_fail(e, "ticc_debug_tc_update: shared memory");
+  int dev = 0, sms = 0;
+  e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return cuda_fail(e, "ticc_debug_tc_update: device");
+  const int blocks = n_tiles < sms ? n_tiles : sms;
+  ticc::tc_tiles_kernel<<<blocks, 256, ticc::kTcSmemBytes, s>>>(maps, tiles, n_tiles, flag, device_status);
+  ticc::note_launch();
+  e = cudaGetLastError();
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_debug_tc_update");
 }
 
 // ---- test hook: bounded waits ------------------------------------------------------------------

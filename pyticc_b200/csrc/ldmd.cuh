@@ -45,6 +45,7 @@ struct LdmdLayout {
   double* scratch;
   size_t scratch_doubles;
   int* reduced;   // [n_sector] leading sweep blocks taken in TF32x3 (mixed mode), else null
+  float* split;   // TF32 hi/lo panels of the reduced steps' tcgen05 update (mixed mode), else null
 };
 
 // Mixed precision: a channel whose local wavenumber at the sector midpoint exceeds this
@@ -427,11 +428,11 @@ inline cudaError_t ldmd_propagate(double* Y, const double* energies, double mu, 
   for (int s = 0; s < sec.n_sector; ++s) {
     ldmd_elementwise_kernel<<<grid, 256, 0, stream>>>(s == 0 ? 0 : 1, s, sec, L, Y, Y);
     note_launch();
-    err = sweep_sym(L.M, mstride, L.np, batch, L.scratch, status, stream, L.reduced ? L.reduced + s : nullptr, used);
+    err = sweep_sym(L.M, mstride, L.np, batch, L.scratch, status, stream, L.reduced ? L.reduced + s : nullptr, used, L.split);
     if (err != cudaSuccess) return err;
     ldmd_elementwise_kernel<<<grid, 256, 0, stream>>>(2, s, sec, L, Y, Y);
     note_launch();
-    err = sweep_sym(L.M, mstride, L.np, batch, L.scratch, status, stream, L.reduced ? L.reduced + s : nullptr, used);
+    err = sweep_sym(L.M, mstride, L.np, batch, L.scratch, status, stream, L.reduced ? L.reduced + s : nullptr, used, L.split);
     if (err != cudaSuccess) return err;
   }
   ldmd_elementwise_kernel<<<grid, 256, 0, stream>>>(3, sec.n_sector - 1, sec, L, Y, Y);

@@ -24,6 +24,7 @@
 #pragma once
 
 #include "dmma_tile.cuh"
+#include "tc_update.cuh"
 #include "ticc_common.cuh"
 
 namespace ticc {
@@ -683,7 +684,9 @@ __device__ inline bool step_wait(const int* f0, const int* f1, int target, int* 
 // matrix's P^-1 for the step.  When the
 // pivot block K is strongly closed (`reduced`), U takes the same FP32-accurate TF32x3
 // product as the step's trailing update.
-__device__ inline void rowpanel_unit(double* Mb, int ld, int kb, int jt, const double* Pt, double* Cb, double* smem, bool reduced) {
+// With `split` (a reduced step whose trailing update runs on tcgen05), the old rows and U of
+// this column tile also go out split into TF32 hi/lo words for the update's TMA loads.
+__device__ inline void rowpanel_unit(double* Mb, int ld, int kb, int jt, const double* Pt, double* Cb, double* smem, bool reduced, float* split, int b) {
   const int k0 = kb * kBlock, c0 = jt * kBlock;
   load_cold_tile(Cb, ld, Mb, kb, jt, smem);
   if (reduced) {
@@ -697,6 +700,11 @@ __device__ inline void rowpanel_unit(double* Mb, int ld, int kb, int jt, const d
   }
   __syncthreads();
   store_tile(Mb, ld, k0, c0, smem);
+  if (split != nullptr) {
+    tc_write_split(split, b, 0, ld, Cb, ld, c0, c0);          // A = the old rows K
+    tc_write_split(split, b, 2, ld, smem, kStride, 0, c0);    // B = U = P^-1 (old rows K)
+    fence_proxy_async_global();                               // read next by TMA (async proxy)
+  }
 }
 
 template <class Acc>
@@ -720,10 +728,19 @@ __device__ inline void update_unit_split(double* Mb, int ld, int k0, int r0, int
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kGemmThreads, 1) sweep_step_kernel(double* __restrict__ M, long long mstride, int ld, int kb, double* __restrict__ cold, long long cstride, int t, int batch, int fuse_next, double* __restrict__ pinv, int* status, const int* __restrict__ reduced_blocks, int* ints) {
+// Dynamic shared memory of the step kernel: the FP64 units use the first kUpdTileSmemBytes,
+// a reduced step's tcgen05 units the first kTcSmemBytes; the unit queue's broadcast slot
+// sits after both.
+constexpr size_t kStepSlotOffset = (size_t(kTcSmemBytes) > kUpdTileSmemBytes ? size_t(kTcSmemBytes) : kUpdTileSmemBytes);
+constexpr size_t kStepSmemBytes = kStepSlotOffset + 16;
+
+// In a reduced step with `split` (and tensor maps over it and M), the trailing-update tiles
+// run on the tcgen05 tensor core (tc_update_unit); otherwise on the mma.sync paths.
+__global__ void __launch_bounds__(kGemmThreads, 1) sweep_step_kernel(double* __restrict__ M, long long mstride, int ld, int kb, double* __restrict__ cold, long long cstride, int t, int batch, int fuse_next, double* __restrict__ pinv, int* status, const int* __restrict__ reduced_blocks, int* ints,
+                                                                     float* __restrict__ split, const __grid_constant__ TcMaps maps) {
   extern __shared__ double smem[];
   const int tid = threadIdx.x;
-  int* slot = reinterpret_cast<int*>(smem + kUpdStageDoubles + kBlock * kStride);
+  int* slot = reinterpret_cast<int*>(reinterpret_cast<char*>(smem) + kStepSlotOffset);
   int* queue = ints + (kb & 1);
   int* abort_flag = ints + 2;
   if (blockIdx.x == 0 && tid == 0) ints[(kb + 1) & 1] = 0;  // the next step's queue
@@ -734,6 +751,13 @@ __global__ void __launch_bounds__(kGemmThreads, 1) sweep_step_kernel(double* __r
   const int k0 = kb * kBlock;
   const int pslot = kb & 1, nslot = (kb + 1) & 1;
   const bool reduced = reduced_blocks != nullptr && kb < *reduced_blocks;
+  const bool tensor_core = reduced && split != nullptr;
+  TcState tcs;
+  bool tc_live = false;
+  if (tensor_core) {
+    tc_setup(tcs, smem);
+    tc_live = true;
+  }
   for (;;) {
     if (tid == 0) *slot = atomicAdd(queue, 1);
     __syncthreads();
@@ -744,7 +768,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) sweep_step_kernel(double* __r
       const int b = u / t, j = u % t;
       const int jt = j + (j >= kb ? 1 : 0);
       double* Mb = M + (long long)b * mstride;
-      rowpanel_unit(Mb, ld, kb, jt, pinv + (long long)b * 2 * kBlock * kBlock + pslot * kBlock * kBlock, cold + (long long)b * cstride, smem, reduced);
+      rowpanel_unit(Mb, ld, kb, jt, pinv + (long long)b * 2 * kBlock * kBlock + pslot * kBlock * kBlock, cold + (long long)b * cstride, smem, reduced, tensor_core ? split : nullptr, b);
       __syncthreads();
       if (tid == 0) {
         __threadfence();
@@ -790,13 +814,17 @@ __global__ void __launch_bounds__(kGemmThreads, 1) sweep_step_kernel(double* __r
     if (!step_wait(fa, fb, kb + 1, abort_flag, status, b, slot)) continue;
     double* Mb = M + (long long)b * mstride;
     const double* Cb = cold + (long long)b * cstride;
-    if (reduced) {
+    if (tensor_core) {
+      // after a failed unit this CTA's tensor-core state is unknown: it only drains the queue
+      if (tc_live && !tc_update_unit(tcs, maps, b, ta, tb, abort_flag, status)) tc_live = false;
+    } else if (reduced) {
       update_unit_split(Mb, ld, k0, ta * kBlock, tb * kBlock, Cb, smem);
     } else {
       TileAcc acc;
       update_unit(acc, Mb, ld, k0, ta * kBlock, tb * kBlock, Cb, smem);
     }
   }
+  if (tensor_core) tc_teardown(tcs);
 }
 
 // Scratch per matrix: cold (kBlock x np) + P^-1 and its transpose (2 x kBlock x kBlock).
@@ -814,7 +842,7 @@ inline cudaError_t sweep_configure_variant() {
   return cudaFuncSetAttribute(sweep_update_kernel<kSym>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmemBytes);
 }
 
-inline cudaError_t sweep_configure_step() { return cudaFuncSetAttribute(sweep_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmemBytes); }
+inline cudaError_t sweep_configure_step() { return cudaFuncSetAttribute(sweep_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStepSmemBytes); }
 
 inline cudaError_t sweep_configure() {
   // per-device attribute: cheap to repeat, so no process-wide cache is kept
@@ -831,8 +859,11 @@ inline cudaError_t sweep_configure() {
 // M <- -M^{-1}.  scratch holds batch * sweep_scratch_doubles(np) doubles.
 // Launches: one pivot kernel, then per block a row panel (and column panel for the
 // general sweep) and an update that also inverts the next pivot block.
+// With reduced_blocks and `split` (tc_split_floats(np, batch) floats, 16-byte aligned), the
+// reduced steps' trailing updates run on the tcgen05 tensor core.
 template <bool kSym>
-inline cudaError_t sweep_batched(double* M, long long mstride, int np, int batch, double* scratch, int* status, cudaStream_t stream, const int* reduced_blocks = nullptr, int n_used = 0) {
+inline cudaError_t sweep_batched(double* M, long long mstride, int np, int batch, double* scratch, int* status, cudaStream_t stream, const int* reduced_blocks = nullptr, int n_used = 0,
+                                 float* split = nullptr) {
   cudaError_t e = sweep_configure();
   if (e != cudaSuccess) return e;
   const int nt = np / kBlock;
@@ -860,13 +891,19 @@ inline cudaError_t sweep_batched(double* M, long long mstride, int np, int batch
   sweep_pivot_kernel<kSym><<<batch, kPivotThreads, kPivotSmemBytes, stream>>>(M, mstride, np, 0, pinv, status);
   note_launch();
   if (fused) {
+    TcMaps maps{};
+    float* tc_split = (reduced_blocks != nullptr) ? split : nullptr;
+    if (tc_split != nullptr) {
+      e = tc_make_maps(maps, tc_split, M, np, mstride, batch);
+      if (e != cudaSuccess) return e;
+    }
     const int t = nt - 1;
     const long long per = (long long)t * (t + 1) / 2;
     for (int kb = 0; kb < nt; ++kb) {
       const int fuse = (kb + 1 < nt) ? 1 : 0;
       const long long work = (long long)t * batch + (fuse ? batch : 0) + per * batch;
       const long long blocks = work < sms ? work : sms;
-      sweep_step_kernel<<<(unsigned)blocks, kGemmThreads, kUpdateSmemBytes, stream>>>(M, mstride, np, kb, cold, cstride, t, batch, fuse, pinv, status, reduced_blocks, queue);
+      sweep_step_kernel<<<(unsigned)blocks, kGemmThreads, kStepSmemBytes, stream>>>(M, mstride, np, kb, cold, cstride, t, batch, fuse, pinv, status, reduced_blocks, queue, tc_split, maps);
       note_launch();
     }
     return cudaGetLastError();
@@ -893,8 +930,9 @@ inline cudaError_t sweep_batched(double* M, long long mstride, int np, int batch
 }
 
 // n_used > 0 states that only the leading n_used rows and columns differ from the identity.
-inline cudaError_t sweep_sym(double* M, long long mstride, int np, int batch, double* scratch, int* status, cudaStream_t stream, const int* reduced_blocks = nullptr, int n_used = 0) {
-  return sweep_batched<true>(M, mstride, np, batch, scratch, status, stream, reduced_blocks, n_used);
+inline cudaError_t sweep_sym(double* M, long long mstride, int np, int batch, double* scratch, int* status, cudaStream_t stream, const int* reduced_blocks = nullptr, int n_used = 0,
+                             float* split = nullptr) {
+  return sweep_batched<true>(M, mstride, np, batch, scratch, status, stream, reduced_blocks, n_used, split);
 }
 inline cudaError_t sweep_general(double* M, long long mstride, int np, int batch, double* scratch, int* status, cudaStream_t stream) {
   return sweep_batched<false>(M, mstride, np, batch, scratch, status, stream);

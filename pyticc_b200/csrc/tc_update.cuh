@@ -1,0 +1,430 @@
+// TF32x3 trailing-update tiles on the 5th-generation tensor core (tcgen05 + TMA + TMEM).
+//
+// One unit computes C <- C - A^T B for a 128 x 128 FP64 tile C of a work matrix, with
+// A = the old pivot rows (cold, 128 x 128 block of columns ta) and B = U = P^-1 cold
+// (columns tb), both given pre-split as x = hi + lo in TF32 (FP32 words):
+//   D = A_lo B_hi + A_hi B_lo + A_hi B_hi      (FP32 accumulation in TMEM, ~2^-21 relative)
+// Operands arrive by TMA (cp.async.bulk.tensor, 128-byte swizzle, MN-major canonical
+// layout) through a ring of kTcStages shared-memory stages of kTcChunk k-rows; one thread
+// issues tcgen05.mma.cta_group::1.kind::tf32 (M = N = 128, K = 8 per instruction) into a
+// 128-column TMEM accumulator and commits to mbarriers that free the stages.  The FP64 C
+// tile is loaded by TMA into shared memory while the products run, C - D is formed there
+// (D read from TMEM with tcgen05.ld, one TMEM lane = one row), and the tile goes back by
+// TMA store.  A diagonal tile is symmetrised from its lower half before the store.
+//
+// Split panel layout in global memory (written by the row-panel units, read by TMA):
+//   float split[batch][4][np / 32][128][32],  which = 0: A_hi, 1: A_lo, 2: B_hi, 3: B_lo,
+// element (k, c) of panel `which` of matrix b at (((b * 4 + which) * (np/32) + c/32) * 128 + k) * 32 + c % 32,
+// so that a TMA box {32, kTcChunk, 4, 1} lands one stage array as [4 mn-atoms][kTcChunk k][32].
+//
+// Every mbarrier wait is bounded (kTcSpinLimit polls, about a second); on a timeout the unit
+// raises the call's abort flag, reports kDeviceStalled, waits (bounded again) for the loads
+// and products it issued, and the CTA frees its TMEM before it exits.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "ticc_common.cuh"
+
+namespace ticc {
+
+constexpr int kTcChunk = 16;                                       // k rows per stage
+constexpr int kTcStages = 3;
+constexpr int kTcArrayBytes = kBlock * kTcChunk * 4;               // 8 KB: one of A_hi, A_lo, B_hi, B_lo
+constexpr int kTcStageBytes = 4 * kTcArrayBytes;                   // 32 KB
+constexpr int kTcCBytes = kBlock * kBlock * 8;                     // 128 KB FP64 C tile (8 chunks of 16 columns)
+constexpr int kTcCChunkBytes = kBlock * 16 * 8;                    // 16 KB
+constexpr int kTcStageOffset = kTcCBytes;
+constexpr int kTcBarOffset = kTcStageOffset + kTcStages * kTcStageBytes;  // 229376
+constexpr int kTcFull = 0, kTcEmpty = kTcStages, kTcAcc = 2 * kTcStages, kTcCFull = 2 * kTcStages + 1, kTcDrain = 2 * kTcStages + 2;
+constexpr int kTcBarriers = 2 * kTcStages + 3;
+constexpr int kTcTmemSlotOffset = kTcBarOffset + 8 * kTcBarriers;
+constexpr int kTcRegionBytes = kTcTmemSlotOffset + 16;
+constexpr int kTcSmemBytes = kTcRegionBytes + 1024;                // + alignment slack of the dynamic base
+constexpr int kTcTmemColumns = 128;
+constexpr long long kTcSpinLimit = 1LL << 20;                      // try_wait polls (each may suspend briefly): about a second
+// instruction descriptor: D F32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12 = 2), A and B
+// MN-major (bits 15, 16), N = 128 (bits 17-22 = N >> 3), M = 128 (bits 24-28 = M >> 4)
+constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(kBlock >> 3) << 17) | ((uint32_t)(kBlock >> 4) << 24);
+static_assert(kTcRegionBytes + 1024 <= 232448, "tcgen05 update region must fit the 227 KB shared-memory limit");
+
+// ---- PTX wrappers ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) { asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory"); }
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the phase of parity `parity` to complete.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (long long it = 0; it < kTcSpinLimit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void fence_proxy_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
+  asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+               "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, int w, uint32_t bar) {
+  asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+               "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, uint32_t src, int x, int y, int z) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(reinterpret_cast<uint64_t>(map)), "r"(src), "r"(x), "r"(y),
+               "r"(z)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t slot, uint32_t columns) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(columns) : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() { asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t columns) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(columns) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_mma_tf32(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tc_ld_16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared-memory matrix descriptor of one MN-major, 128-byte-swizzled stage array: 4 atoms of
+// 32 mn values along M/N (LBO = kTcChunk * 128 bytes apart), 8-row k groups 1024 bytes apart
+// (SBO); `kgroup` selects the 8 k rows of one instruction.
+__device__ __forceinline__ uint64_t tc_desc(uint32_t array_addr, int kgroup) {
+  const uint32_t start = array_addr + (uint32_t)kgroup * 1024u;
+  uint64_t d = 0;
+  d |= (uint64_t)((start >> 4) & 0x3FFFu);
+  d |= (uint64_t)(((kTcChunk * 128u) >> 4) & 0x3FFFu) << 16;  // LBO: next 32-wide mn atom
+  d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 32;             // SBO: next 8-row k group
+  d |= (uint64_t)1 << 46;                                     // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;                                     // 128-byte swizzle
+  return d;
+}
+
+// Byte offset of C(r, j) inside the shared C tile: 8 chunks of 16 columns, each 128 rows of
+// 128 bytes with the 128-byte swizzle TMA applies (16-byte unit index XOR row % 8).
+__device__ __forceinline__ int tc_c_offset(int r, int j) { return (j >> 4) * kTcCChunkBytes + r * 128 + ((((j & 15) >> 1) ^ (r & 7)) << 4) + (j & 1) * 8; }
+
+// Per-CTA state of the tcgen05 unit: the aligned region, its barriers, TMEM and the running
+// chunk / tile counters that give every barrier wait its phase parity.
+struct TcState {
+  char* base;       // 1024-aligned start of the region
+  uint32_t base_u;  // its shared-window address
+  uint32_t tmem;    // accumulator (lane 0, first column)
+  uint32_t chunk;   // operand chunks issued so far (thread 0's count)
+  uint32_t tile;    // tiles finished so far
+};
+
+__device__ __forceinline__ uint32_t tc_bar(const TcState& s, int i) { return s.base_u + kTcBarOffset + 8u * (uint32_t)i; }
+
+// Set up the region (thread 0 initialises the barriers, warp 0 allocates TMEM).  Every
+// thread of the CTA calls it once, before the first unit.
+__device__ inline void tc_setup(TcState& s, void* dynamic_smem) {
+  const uintptr_t raw = reinterpret_cast<uintptr_t>(dynamic_smem);
+  const uint32_t raw_u = smem_u32(dynamic_smem);
+  const uint32_t pad = (1024u - (raw_u & 1023u)) & 1023u;
+  s.base = reinterpret_cast<char*>(raw + pad);
+  s.base_u = raw_u + pad;
+  s.chunk = 0;
+  s.tile = 0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kTcBarriers; ++i) mbar_init(tc_bar(s, i), 1);
+    mbar_fence_init();
+  }
+  if (threadIdx.x < 32) {
+    tmem_alloc(s.base_u + kTcTmemSlotOffset, kTcTmemColumns);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  s.tmem = *reinterpret_cast<volatile uint32_t*>(s.base + kTcTmemSlotOffset);
+}
+
+// Free TMEM; every thread calls it once, after its last unit (and after any failure).
+__device__ inline void tc_teardown(TcState& s) {
+  if (threadIdx.x == 0) bulk_wait_all();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (threadIdx.x < 32) tmem_dealloc(s.tmem, kTcTmemColumns);
+}
+
+struct TcMaps {
+  CUtensorMap split;   // 4-D over the split panels (see the header comment)
+  CUtensorMap matrix;  // 3-D {np, np, batch} over the FP64 work matrices, box {16, 128, 1}
+};
+
+// Issue the four TMA loads of operand chunk `c` (k rows c * kTcChunk ..) of tile (ta, tb) of
+// matrix b into stage `stage`; thread 0 only.
+__device__ __forceinline__ void tc_issue_chunk(const TcState& s, const CUtensorMap* split, int b, int ta, int tb, int c, int stage) {
+  const uint32_t dst = s.base_u + kTcStageOffset + (uint32_t)stage * kTcStageBytes;
+  const uint32_t full = tc_bar(s, kTcFull + stage);
+  mbar_expect_tx(full, kTcStageBytes);
+  const int k0 = c * kTcChunk;
+  tma_load_4d(dst + 0 * kTcArrayBytes, split, 0, k0, 4 * ta, 4 * b + 0, full);
+  tma_load_4d(dst + 1 * kTcArrayBytes, split, 0, k0, 4 * ta, 4 * b + 1, full);
+  tma_load_4d(dst + 2 * kTcArrayBytes, split, 0, k0, 4 * tb, 4 * b + 2, full);
+  tma_load_4d(dst + 3 * kTcArrayBytes, split, 0, k0, 4 * tb, 4 * b + 3, full);
+}
+
+// One update tile.  Returns false (on every thread) if a wait gave up; the abort flag and
+// status are then set and the unit's issued work has been drained (bounded waits).
+__device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int ta, int tb, int* abort_flag, int* status) {
+  constexpr int nchunks = kBlock / kTcChunk;  // 8
+  __shared__ int tc_ok;
+  const int tid = threadIdx.x;
+  const int r0 = ta * kBlock, c0 = tb * kBlock;
+  if (tid == 0) {
+    int ok = 1;
+    unsigned loads_pending = 0;  // stages whose TMA load was issued and not yet waited
+    uint32_t pending_parity[kTcStages] = {};
+    bool c_pending = false, mma_issued = false;
+    // the C tile: the previous unit's generic accesses of the buffer are ordered before this
+    // load by the barrier that ended it and this proxy fence; split panels written by other
+    // CTAs of this launch were released to this thread by the flag it acquired
+    fence_proxy_async_shared();
+    fence_proxy_async_global();
+    const uint32_t cbar = tc_bar(s, kTcCFull);
+    mbar_expect_tx(cbar, kTcCBytes);
+    for (int q = 0; q < 8; ++q) tma_load_3d(s.base_u + (uint32_t)q * kTcCChunkBytes, &maps.matrix, c0 + 16 * q, r0, b, cbar);
+    c_pending = true;
+    // operand ring: chunk g = s.chunk + c uses stage g % kTcStages in its (g / kTcStages)-th use
+    const uint32_t g0 = s.chunk;
+    auto issue = [&](int c, uint32_t g) {
+      const int stage = g % kTcStages;
+      tc_issue_chunk(s, &maps.split, b, ta, tb, c, stage);
+      loads_pending |= 1u << stage;
+      pending_parity[stage] = (g / kTcStages) & 1u;
+    };
+    for (int c = 0; c < kTcStages && c < nchunks && ok; ++c) {
+      const uint32_t g = g0 + c;
+      // the MMAs that last read this stage (chunk g - kTcStages) have completed
+      if (g >= (uint32_t)kTcStages && !mbar_wait(tc_bar(s, kTcEmpty + g % kTcStages), ((g - kTcStages) / kTcStages) & 1u)) ok = 0;
+      if (ok) issue(c, g);
+    }
+    tc_fence_after();
+    for (int c = 0; c < nchunks && ok; ++c) {
+      const uint32_t g = g0 + c;
+      const int stage = g % kTcStages;
+      if (!mbar_wait(tc_bar(s, kTcFull + stage), (g / kTcStages) & 1u)) {
+        ok = 0;
+        break;
+      }
+      loads_pending &= ~(1u << stage);
+      tc_fence_after();
+      const uint32_t st = s.base_u + kTcStageOffset + (uint32_t)stage * kTcStageBytes;
+#pragma unroll
+      for (int kg = 0; kg < kTcChunk / 8; ++kg) {
+        const uint64_t a_hi = tc_desc(st + 0 * kTcArrayBytes, kg), a_lo = tc_desc(st + 1 * kTcArrayBytes, kg);
+        const uint64_t b_hi = tc_desc(st + 2 * kTcArrayBytes, kg), b_lo = tc_desc(st + 3 * kTcArrayBytes, kg);
+        tc_mma_tf32(s.tmem, a_lo, b_hi, (c > 0 || kg > 0) ? 1u : 0u);
+        tc_mma_tf32(s.tmem, a_hi, b_lo, 1u);
+        tc_mma_tf32(s.tmem, a_hi, b_hi, 1u);
+      }
+      mma_issued = true;
+      tc_commit(tc_bar(s, kTcEmpty + stage));
+      // refill the stage of the previous chunk (its MMAs precede this chunk's in the pipe)
+      if (c >= 1 && c - 1 + kTcStages < nchunks) {
+        const uint32_t gp = g - 1;
+        if (!mbar_wait(tc_bar(s, kTcEmpty + gp % kTcStages), (gp / kTcStages) & 1u)) {
+          ok = 0;
+          break;
+        }
+        issue(c - 1 + kTcStages, gp + kTcStages);
+      }
+    }
+    if (ok) {
+      tc_commit(tc_bar(s, kTcAcc));
+      s.chunk = g0 + nchunks;
+      mma_issued = false;
+      if (!mbar_wait(tc_bar(s, kTcAcc), s.tile & 1u)) ok = 0;
+      if (ok && mbar_wait(cbar, s.tile & 1u)) c_pending = false;
+      else ok = 0;
+    }
+    if (!ok) {
+      if (atomicExch(abort_flag, 1) == 0) report_status(status, kDeviceStalled, b, -1);
+      // drain: the issued loads and products land before the CTA moves on or frees TMEM
+      for (int st = 0; st < kTcStages; ++st)
+        if (loads_pending & (1u << st)) mbar_wait(tc_bar(s, kTcFull + st), pending_parity[st]);
+      if (c_pending) mbar_wait(cbar, s.tile & 1u);
+      if (mma_issued) {
+        tc_commit(tc_bar(s, kTcDrain));
+        mbar_wait(tc_bar(s, kTcDrain), 0u);
+      }
+    }
+    tc_ok = ok;
+  }
+  __syncthreads();
+  if (!tc_ok) return false;
+  // every thread observes the completed C load itself (acquire of the async-proxy writes)
+  mbar_wait(tc_bar(s, kTcCFull), s.tile & 1u);
+  tc_fence_after();
+  // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (one row each), columns of half w / 4
+  const int warp = tid >> 5, lane = tid & 31;
+  const int r = 32 * (warp & 3) + lane;
+  const int half = warp >> 2;
+#pragma unroll 1
+  for (int q = 0; q < 4; ++q) {
+    const int col = 64 * half + 16 * q;
+    float d[16];
+    tc_ld_16(s.tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)col, d);
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      double2* p = reinterpret_cast<double2*>(s.base + tc_c_offset(r, col + 2 * u));
+      double2 v = *p;
+      v.x -= (double)d[2 * u];
+      v.y -= (double)d[2 * u + 1];
+      *p = v;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (ta == tb) {  // keep a diagonal tile exactly symmetric: upper half from the lower half
+    for (int e = tid; e < kBlock * kBlock; e += blockDim.x) {
+      const int rr = e >> 7, cc = e & (kBlock - 1);
+      if (rr < cc) *reinterpret_cast<double*>(s.base + tc_c_offset(rr, cc)) = *reinterpret_cast<const double*>(s.base + tc_c_offset(cc, rr));
+    }
+    __syncthreads();
+  }
+  fence_proxy_async_shared();
+  __syncthreads();
+  if (tid == 0) {
+    for (int q = 0; q < 8; ++q) tma_store_3d(&maps.matrix, s.base_u + (uint32_t)q * kTcCChunkBytes, c0 + 16 * q, r0, b);
+    bulk_commit();
+    bulk_wait_read_all();  // the C buffer is reused by the next unit's load
+  }
+  ++s.tile;
+  __syncthreads();
+  return true;
+}
+
+// Element (k, c) of split panel `which` of matrix b.
+__device__ __forceinline__ long long tc_split_index(int b, int which, int np, int k, int c) { return ((((long long)b * 4 + which) * (np >> 5) + (c >> 5)) * kBlock + k) * 32 + (c & 31); }
+
+__device__ __forceinline__ void tc_split_value(double x, float& hi, float& lo) {
+  unsigned h, l;
+  const float f = static_cast<float>(x);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(f));
+  const float rest = f - __uint_as_float(h);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(rest));
+  hi = __uint_as_float(h);
+  lo = __uint_as_float(l);
+}
+
+// Write the split of one 128 x 128 block of a panel (k rows 0..127 of src at row stride ld,
+// columns src_c0 .. src_c0 + 127) into panels which_hi / which_hi + 1 at columns dst_c0 ..
+// dst_c0 + 127.  All threads of the CTA; consecutive threads write consecutive columns.
+__device__ inline void tc_write_split(float* split, int b, int which_hi, int np, const double* src, long long ld, int src_c0, int dst_c0) {
+  for (int e = threadIdx.x; e < kBlock * kBlock; e += blockDim.x) {
+    const int k = e >> 7, c = e & (kBlock - 1);
+    float hi, lo;
+    tc_split_value(src[(long long)k * ld + src_c0 + c], hi, lo);
+    split[tc_split_index(b, which_hi, np, k, dst_c0 + c)] = hi;
+    split[tc_split_index(b, which_hi + 1, np, k, dst_c0 + c)] = lo;
+  }
+}
+
+inline size_t tc_split_floats(int np, int batch) { return size_t(4) * kBlock * (size_t)np * (size_t)batch; }
+
+// ---- host: tensor maps ----------------------------------------------------------------------------
+typedef CUresult (*TcEncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                                   CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+inline TcEncodeTiled tc_encoder() {
+  static TcEncodeTiled fn = []() -> TcEncodeTiled {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess) return nullptr;
+    return reinterpret_cast<TcEncodeTiled>(p);
+  }();
+  return fn;
+}
+
+// Tensor maps over the split panels of `batch` matrices and over the matrices themselves
+// (FP64, row stride np, matrix stride mstride elements).
+inline cudaError_t tc_make_maps(TcMaps& maps, const float* split, const double* M, int np, long long mstride, int batch) {
+  TcEncodeTiled encode = tc_encoder();
+  if (encode == nullptr) return cudaErrorNotSupported;
+  if (np % kBlock != 0 || (reinterpret_cast<uintptr_t>(split) & 15) || (reinterpret_cast<uintptr_t>(M) & 15) || (mstride * 8) % 16 != 0) return cudaErrorInvalidValue;
+  const cuuint64_t sdim[4] = {32, (cuuint64_t)kBlock, (cuuint64_t)(np / 32), (cuuint64_t)(4 * batch)};
+  const cuuint64_t sstride[3] = {32 * 4, (cuuint64_t)kBlock * 32 * 4, (cuuint64_t)(np / 32) * kBlock * 32 * 4};
+  const cuuint32_t sbox[4] = {32, (cuuint32_t)kTcChunk, 4, 1};
+  const cuuint32_t ones[4] = {1, 1, 1, 1};
+  CUresult r = encode(&maps.split, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(split), sdim, sstride, sbox, ones, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  const cuuint64_t mdim[3] = {(cuuint64_t)np, (cuuint64_t)np, (cuuint64_t)batch};
+  const cuuint64_t mstr[2] = {(cuuint64_t)np * 8, (cuuint64_t)mstride * 8};
+  const cuuint32_t mbox[3] = {16, (cuuint32_t)kBlock, 1};
+  r = encode(&maps.matrix, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(M), mdim, mstr, mbox, ones, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+// ---- bring-up path: split two panels, then update a list of tiles ---------------------------------
+// cold and U: [batch][128][np]; one CTA per (128-column block, matrix).
+__global__ void __launch_bounds__(256) tc_split_panels_kernel(const double* cold, const double* U, int np, int batch, float* split) {
+  const int jt = blockIdx.x, b = blockIdx.y;
+  tc_write_split(split, b, 0, np, cold + (long long)b * kBlock * np, np, jt * kBlock, jt * kBlock);
+  tc_write_split(split, b, 2, np, U + (long long)b * kBlock * np, np, jt * kBlock, jt * kBlock);
+}
+
+// tiles[3 t .. 3 t + 2] = (matrix, row tile, column tile); every CTA takes tiles t = blockIdx.x,
+// blockIdx.x + gridDim.x, ...
+__global__ void __launch_bounds__(256, 1) tc_tiles_kernel(const __grid_constant__ TcMaps maps, const int* tiles, int n_tiles, int* abort_flag, int* status) {
+  extern __shared__ __align__(1024) char tc_smem[];
+  TcState s;
+  tc_setup(s, tc_smem);
+  for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    if (!tc_update_unit(s, maps, tiles[3 * t], tiles[3 * t + 1], tiles[3 * t + 2], abort_flag, status)) break;
+  }
+  tc_teardown(s);
+}
+
+}  // namespace ticc
