@@ -515,7 +515,7 @@ int ticc_debug_tc_update(double* M, int np, int batch, const double* cold, const
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return cuda_fail(e, "ticc_debug_tc_update: device");
   const int blocks = n_tiles < sms ? n_tiles : sms;
-  ticc::tc_tiles_kernel<<<blocks, 256, ticc::kTcSmemBytes, s>>>(maps, tiles, n_tiles, flag, device_status);
+  ticc::tc_tiles_kernel<<<blocks, 256, ticc::kTcSmemBytes, s>>>(maps, np, tiles, n_tiles, flag, device_status);
   ticc::note_launch();
   e = cudaGetLastError();
   return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_debug_tc_update");

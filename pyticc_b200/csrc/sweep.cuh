@@ -701,8 +701,8 @@ __device__ inline void rowpanel_unit(double* Mb, int ld, int kb, int jt, const d
   __syncthreads();
   store_tile(Mb, ld, k0, c0, smem);
   if (split != nullptr) {
-    tc_write_split(split, b, 0, ld, Cb, ld, c0, c0);          // A = the old rows K
-    tc_write_split(split, b, 2, ld, smem, kStride, 0, c0);    // B = U = P^-1 (old rows K)
+    tc_write_split(split, b, 0, ld, Cb, ld, c0, jt);          // A = the old rows K
+    tc_write_split(split, b, 2, ld, smem, kStride, 0, jt);    // B = U = P^-1 (old rows K)
     fence_proxy_async_global();                               // read next by TMA (async proxy)
   }
 }
@@ -755,7 +755,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) sweep_step_kernel(double* __r
   TcState tcs;
   bool tc_live = false;
   if (tensor_core) {
-    tc_setup(tcs, smem);
+    tc_setup(tcs, smem, ld);
     tc_live = true;
   }
   for (;;) {

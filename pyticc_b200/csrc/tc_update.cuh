@@ -4,18 +4,22 @@
 // A = the old pivot rows (cold, 128 x 128 block of columns ta) and B = U = P^-1 cold
 // (columns tb), both given pre-split as x = hi + lo in TF32 (FP32 words):
 //   D = A_lo B_hi + A_hi B_lo + A_hi B_hi      (FP32 accumulation in TMEM, ~2^-21 relative)
-// Operands arrive by TMA (cp.async.bulk.tensor, 128-byte swizzle, MN-major canonical
-// layout) through a ring of kTcStages shared-memory stages of kTcChunk k-rows; one thread
+// Operands arrive by TMA (cp.async.bulk.tensor) through a ring of kTcStages shared-memory
+// stages of kTcChunk k-rows, already in the canonical K-major no-swizzle layout; one thread
 // issues tcgen05.mma.cta_group::1.kind::tf32 (M = N = 128, K = 8 per instruction) into a
 // 128-column TMEM accumulator and commits to mbarriers that free the stages.  The FP64 C
-// tile is loaded by TMA into shared memory while the products run, C - D is formed there
-// (D read from TMEM with tcgen05.ld, one TMEM lane = one row), and the tile goes back by
-// TMA store.  A diagonal tile is symmetrised from its lower half before the store.
+// tile is loaded by TMA (128-byte swizzle) into shared memory while the products run, C - D
+// is formed there (D read from TMEM with tcgen05.ld, one TMEM lane = one row), and the tile
+// goes back by TMA store.  A diagonal tile is symmetrised from its lower half before the
+// store.
 //
-// Split panel layout in global memory (written by the row-panel units, read by TMA):
-//   float split[batch][4][np / 32][128][32],  which = 0: A_hi, 1: A_lo, 2: B_hi, 3: B_lo,
-// element (k, c) of panel `which` of matrix b at (((b * 4 + which) * (np/32) + c/32) * 128 + k) * 32 + c % 32,
-// so that a TMA box {32, kTcChunk, 4, 1} lands one stage array as [4 mn-atoms][kTcChunk k][32].
+// Split panel layout in global memory (written by the row-panel units, read by TMA), one
+// 8 KB block per (matrix b, panel which, 128-column tile ct, 16-row k chunk kc):
+//   block = ((b * 4 + which) * (np / 128) + ct) * 8 + kc,    which = 0: A_hi, 1: A_lo, 2: B_hi, 3: B_lo
+//   element (k, c), m = c % 128, kk = k % 16, at float block * 2048 + ((m / 8) * 4 + kk / 4) * 32 + (m % 8) * 4 + kk % 4
+// i.e. 8-row x 16-byte core matrices, the four along k 128 bytes apart (LBO), the sixteen
+// 8-row groups along m 512 bytes apart (SBO): the MMA's K-major operand layout, so a block
+// is copied into shared memory as it is.
 //
 // Every mbarrier wait is bounded (kTcSpinLimit polls, about a second); on a timeout the unit
 // raises the call's abort flag, reports kDeviceStalled, waits (bounded again) for the loads
@@ -33,7 +37,8 @@ namespace ticc {
 
 constexpr int kTcChunk = 16;                                       // k rows per stage
 constexpr int kTcStages = 3;
-constexpr int kTcArrayBytes = kBlock * kTcChunk * 4;               // 8 KB: one of A_hi, A_lo, B_hi, B_lo
+constexpr int kTcArrayBytes = kBlock * kTcChunk * 4;               // 8 KB: one of A_hi, A_lo, B_hi, B_lo (one split block)
+constexpr int kTcArrayFloats = kTcArrayBytes / 4;
 constexpr int kTcStageBytes = 4 * kTcArrayBytes;                   // 32 KB
 constexpr int kTcCBytes = kBlock * kBlock * 8;                     // 128 KB FP64 C tile (8 chunks of 16 columns)
 constexpr int kTcCChunkBytes = kBlock * 16 * 8;                    // 16 KB
@@ -47,8 +52,10 @@ constexpr int kTcSmemBytes = kTcRegionBytes + 1024;                // + alignmen
 constexpr int kTcTmemColumns = 128;
 constexpr long long kTcSpinLimit = 1LL << 20;                      // try_wait polls (each may suspend briefly): about a second
 // instruction descriptor: D F32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12 = 2), A and B
-// MN-major (bits 15, 16), N = 128 (bits 17-22 = N >> 3), M = 128 (bits 24-28 = M >> 4)
-constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(kBlock >> 3) << 17) | ((uint32_t)(kBlock >> 4) << 24);
+// K-major (bits 15, 16 clear), N = 128 (bits 17-22 = N >> 3), M = 128 (bits 24-28 = M >> 4)
+constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kBlock >> 3) << 17) | ((uint32_t)(kBlock >> 4) << 24);
+constexpr uint32_t kTcLBO = 128;  // bytes between the k-adjacent core matrices of a split block
+constexpr uint32_t kTcSBO = 512;  // bytes between its 8-row groups
 static_assert(kTcRegionBytes + 1024 <= 232448, "tcgen05 update region must fit the 227 KB shared-memory limit");
 
 // ---- PTX wrappers ---------------------------------------------------------------------------
@@ -83,11 +90,6 @@ __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
   asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
                "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
-               : "memory");
-}
-__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, int w, uint32_t bar) {
-  asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
-               "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(bar)
                : "memory");
 }
 __device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, uint32_t src, int x, int y, int z) {
@@ -132,17 +134,15 @@ __device__ __forceinline__ void tc_ld_16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Shared-memory matrix descriptor of one MN-major, 128-byte-swizzled stage array: 4 atoms of
-// 32 mn values along M/N (LBO = kTcChunk * 128 bytes apart), 8-row k groups 1024 bytes apart
-// (SBO); `kgroup` selects the 8 k rows of one instruction.
+// Shared-memory matrix descriptor of one K-major, unswizzled stage array (a split block);
+// `kgroup` selects the 8 k values of one instruction (two core matrices, 256 bytes on).
 __device__ __forceinline__ uint64_t tc_desc(uint32_t array_addr, int kgroup) {
-  const uint32_t start = array_addr + (uint32_t)kgroup * 1024u;
+  const uint32_t start = array_addr + (uint32_t)kgroup * 2u * kTcLBO;
   uint64_t d = 0;
   d |= (uint64_t)((start >> 4) & 0x3FFFu);
-  d |= (uint64_t)(((kTcChunk * 128u) >> 4) & 0x3FFFu) << 16;  // LBO: next 32-wide mn atom
-  d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 32;             // SBO: next 8-row k group
-  d |= (uint64_t)1 << 46;                                     // descriptor version (sm_100)
-  d |= (uint64_t)2 << 61;                                     // 128-byte swizzle
+  d |= (uint64_t)((kTcLBO >> 4) & 0x3FFFu) << 16;  // LBO: next core matrix along k
+  d |= (uint64_t)((kTcSBO >> 4) & 0x3FFFu) << 32;  // SBO: next 8-row group along m / n
+  d |= (uint64_t)1 << 46;                          // descriptor version (sm_100); no swizzle
   return d;
 }
 
@@ -158,13 +158,17 @@ struct TcState {
   uint32_t tmem;    // accumulator (lane 0, first column)
   uint32_t chunk;   // operand chunks issued so far (thread 0's count)
   uint32_t tile;    // tiles finished so far
+  int nt;           // 128-column tiles per matrix (np / 128)
 };
+
+// Split block of (matrix b, panel which, column tile ct, k chunk kc) when a matrix has nt tiles.
+__device__ __forceinline__ int tc_split_block(int b, int which, int nt, int ct, int kc) { return ((b * 4 + which) * nt + ct) * (kBlock / kTcChunk) + kc; }
 
 __device__ __forceinline__ uint32_t tc_bar(const TcState& s, int i) { return s.base_u + kTcBarOffset + 8u * (uint32_t)i; }
 
 // Set up the region (thread 0 initialises the barriers, warp 0 allocates TMEM).  Every
 // thread of the CTA calls it once, before the first unit.
-__device__ inline void tc_setup(TcState& s, void* dynamic_smem) {
+__device__ inline void tc_setup(TcState& s, void* dynamic_smem, int np) {
   const uintptr_t raw = reinterpret_cast<uintptr_t>(dynamic_smem);
   const uint32_t raw_u = smem_u32(dynamic_smem);
   const uint32_t pad = (1024u - (raw_u & 1023u)) & 1023u;
@@ -172,6 +176,7 @@ __device__ inline void tc_setup(TcState& s, void* dynamic_smem) {
   s.base_u = raw_u + pad;
   s.chunk = 0;
   s.tile = 0;
+  s.nt = np / kBlock;
   if (threadIdx.x == 0) {
     for (int i = 0; i < kTcBarriers; ++i) mbar_init(tc_bar(s, i), 1);
     mbar_fence_init();
@@ -196,7 +201,7 @@ __device__ inline void tc_teardown(TcState& s) {
 }
 
 struct TcMaps {
-  CUtensorMap split;   // 4-D over the split panels (see the header comment)
+  CUtensorMap split;   // 3-D {256, 8, blocks} over the split blocks, box {256, 8, 1} (one block)
   CUtensorMap matrix;  // 3-D {np, np, batch} over the FP64 work matrices, box {16, 128, 1}
 };
 
@@ -206,11 +211,11 @@ __device__ __forceinline__ void tc_issue_chunk(const TcState& s, const CUtensorM
   const uint32_t dst = s.base_u + kTcStageOffset + (uint32_t)stage * kTcStageBytes;
   const uint32_t full = tc_bar(s, kTcFull + stage);
   mbar_expect_tx(full, kTcStageBytes);
-  const int k0 = c * kTcChunk;
-  tma_load_4d(dst + 0 * kTcArrayBytes, split, 0, k0, 4 * ta, 4 * b + 0, full);
-  tma_load_4d(dst + 1 * kTcArrayBytes, split, 0, k0, 4 * ta, 4 * b + 1, full);
-  tma_load_4d(dst + 2 * kTcArrayBytes, split, 0, k0, 4 * tb, 4 * b + 2, full);
-  tma_load_4d(dst + 3 * kTcArrayBytes, split, 0, k0, 4 * tb, 4 * b + 3, full);
+  const int nt = s.nt;
+  tma_load_3d(dst + 0 * kTcArrayBytes, split, 0, 0, tc_split_block(b, 0, nt, ta, c), full);
+  tma_load_3d(dst + 1 * kTcArrayBytes, split, 0, 0, tc_split_block(b, 1, nt, ta, c), full);
+  tma_load_3d(dst + 2 * kTcArrayBytes, split, 0, 0, tc_split_block(b, 2, nt, tb, c), full);
+  tma_load_3d(dst + 3 * kTcArrayBytes, split, 0, 0, tc_split_block(b, 3, nt, tb, c), full);
 }
 
 // One update tile.  Returns false (on every thread) if a wait gave up; the abort flag and
@@ -344,9 +349,6 @@ __device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int
   return true;
 }
 
-// Element (k, c) of split panel `which` of matrix b.
-__device__ __forceinline__ long long tc_split_index(int b, int which, int np, int k, int c) { return ((((long long)b * 4 + which) * (np >> 5) + (c >> 5)) * kBlock + k) * 32 + (c & 31); }
-
 __device__ __forceinline__ void tc_split_value(double x, float& hi, float& lo) {
   unsigned h, l;
   const float f = static_cast<float>(x);
@@ -358,15 +360,23 @@ __device__ __forceinline__ void tc_split_value(double x, float& hi, float& lo) {
 }
 
 // Write the split of one 128 x 128 block of a panel (k rows 0..127 of src at row stride ld,
-// columns src_c0 .. src_c0 + 127) into panels which_hi / which_hi + 1 at columns dst_c0 ..
-// dst_c0 + 127.  All threads of the CTA; consecutive threads write consecutive columns.
-__device__ inline void tc_write_split(float* split, int b, int which_hi, int np, const double* src, long long ld, int src_c0, int dst_c0) {
-  for (int e = threadIdx.x; e < kBlock * kBlock; e += blockDim.x) {
-    const int k = e >> 7, c = e & (kBlock - 1);
-    float hi, lo;
-    tc_split_value(src[(long long)k * ld + src_c0 + c], hi, lo);
-    split[tc_split_index(b, which_hi, np, k, dst_c0 + c)] = hi;
-    split[tc_split_index(b, which_hi + 1, np, k, dst_c0 + c)] = lo;
+// columns src_c0 .. src_c0 + 127) into panels which_hi / which_hi + 1, column tile ct.  All
+// threads of the CTA; a thread takes 4 consecutive k of one column (coalesced loads across
+// the warp's consecutive columns) and stores them as one 16-byte row of a core matrix.
+__device__ inline void tc_write_split(float* split, int b, int which_hi, int np, const double* src, long long ld, int src_c0, int ct) {
+  const int nt = np / kBlock;
+  for (int e = threadIdx.x; e < kBlock * (kBlock / 4); e += blockDim.x) {
+    const int k4 = e / kBlock, m = e % kBlock;
+    const int k = 4 * k4;
+    float hi[4], lo[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) tc_split_value(src[(long long)(k + j) * ld + src_c0 + m], hi[j], lo[j]);
+    const int kk = k % kTcChunk;
+    const long long inner = ((m >> 3) * 4 + (kk >> 2)) * 32 + (m & 7) * 4;
+    const long long bh = (long long)tc_split_block(b, which_hi, nt, ct, k / kTcChunk) * kTcArrayFloats;
+    const long long bl = (long long)tc_split_block(b, which_hi + 1, nt, ct, k / kTcChunk) * kTcArrayFloats;
+    *reinterpret_cast<float4*>(split + bh + inner) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<float4*>(split + bl + inner) = make_float4(lo[0], lo[1], lo[2], lo[3]);
   }
 }
 
@@ -392,12 +402,13 @@ inline cudaError_t tc_make_maps(TcMaps& maps, const float* split, const double* 
   TcEncodeTiled encode = tc_encoder();
   if (encode == nullptr) return cudaErrorNotSupported;
   if (np % kBlock != 0 || (reinterpret_cast<uintptr_t>(split) & 15) || (reinterpret_cast<uintptr_t>(M) & 15) || (mstride * 8) % 16 != 0) return cudaErrorInvalidValue;
-  const cuuint64_t sdim[4] = {32, (cuuint64_t)kBlock, (cuuint64_t)(np / 32), (cuuint64_t)(4 * batch)};
-  const cuuint64_t sstride[3] = {32 * 4, (cuuint64_t)kBlock * 32 * 4, (cuuint64_t)(np / 32) * kBlock * 32 * 4};
-  const cuuint32_t sbox[4] = {32, (cuuint32_t)kTcChunk, 4, 1};
+  const cuuint64_t blocks = (cuuint64_t)batch * 4 * (np / kBlock) * (kBlock / kTcChunk);
+  const cuuint64_t sdim[3] = {256, (cuuint64_t)(kTcArrayFloats / 256), blocks};
+  const cuuint64_t sstride[2] = {256 * 4, (cuuint64_t)kTcArrayBytes};
+  const cuuint32_t sbox[3] = {256, (cuuint32_t)(kTcArrayFloats / 256), 1};
   const cuuint32_t ones[4] = {1, 1, 1, 1};
-  CUresult r = encode(&maps.split, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(split), sdim, sstride, sbox, ones, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                      CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult r = encode(&maps.split, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(split), sdim, sstride, sbox, ones, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
   const cuuint64_t mdim[3] = {(cuuint64_t)np, (cuuint64_t)np, (cuuint64_t)batch};
   const cuuint64_t mstr[2] = {(cuuint64_t)np * 8, (cuuint64_t)mstride * 8};
@@ -411,16 +422,16 @@ inline cudaError_t tc_make_maps(TcMaps& maps, const float* split, const double* 
 // cold and U: [batch][128][np]; one CTA per (128-column block, matrix).
 __global__ void __launch_bounds__(256) tc_split_panels_kernel(const double* cold, const double* U, int np, int batch, float* split) {
   const int jt = blockIdx.x, b = blockIdx.y;
-  tc_write_split(split, b, 0, np, cold + (long long)b * kBlock * np, np, jt * kBlock, jt * kBlock);
-  tc_write_split(split, b, 2, np, U + (long long)b * kBlock * np, np, jt * kBlock, jt * kBlock);
+  tc_write_split(split, b, 0, np, cold + (long long)b * kBlock * np, np, jt * kBlock, jt);
+  tc_write_split(split, b, 2, np, U + (long long)b * kBlock * np, np, jt * kBlock, jt);
 }
 
 // tiles[3 t .. 3 t + 2] = (matrix, row tile, column tile); every CTA takes tiles t = blockIdx.x,
 // blockIdx.x + gridDim.x, ...
-__global__ void __launch_bounds__(256, 1) tc_tiles_kernel(const __grid_constant__ TcMaps maps, const int* tiles, int n_tiles, int* abort_flag, int* status) {
+__global__ void __launch_bounds__(256, 1) tc_tiles_kernel(const __grid_constant__ TcMaps maps, int np, const int* tiles, int n_tiles, int* abort_flag, int* status) {
   extern __shared__ __align__(1024) char tc_smem[];
   TcState s;
-  tc_setup(s, tc_smem);
+  tc_setup(s, tc_smem, np);
   for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
     if (!tc_update_unit(s, maps, tiles[3 * t], tiles[3 * t + 1], tiles[3 * t + 2], abort_flag, status)) break;
   }

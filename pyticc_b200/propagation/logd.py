@@ -94,20 +94,27 @@ def propagate_device(Y: torch.Tensor, energies: torch.Tensor, reduced_mass: floa
     return Y
 
 
-def propagate_blocks_device(Y: torch.Tensor, energies: torch.Tensor, reduced_mass: float, half_steps: torch.Tensor, W_start: torch.Tensor, W_mid: torch.Tensor, W_end: torch.Tensor, *, stride, block_stride: int, precision: int = nat.PRECISION_FP64, workspace_slot: int = 0) -> torch.Tensor:
+def blocks_workspace_bytes(n: int, n_energy: int, n_block: int, n_sector: int, is_complex: bool, precision: int) -> int:
+    return nat.size_query(nat.load_library().ticc_ldmd_blocks_workspace_size, n, n_energy, n_block, n_sector, int(is_complex), precision)
+
+
+def propagate_blocks_device(Y: torch.Tensor, energies: torch.Tensor, reduced_mass: float, half_steps: torch.Tensor, W_start: torch.Tensor, W_mid: torch.Tensor, W_end: torch.Tensor, *, stride, block_stride: int, precision: int = nat.PRECISION_FP64, workspace_slot: int = 0, status: "nat.DeviceStatus | None" = None) -> torch.Tensor:
     """Propagate device-resident Y of shape (n_block, n_energy, n, n) in place: block g
     reads its W at element offset g * block_stride from the three W views, whose
     consecutive sectors are ``stride`` elements apart.  Calls that may run concurrently on
-    different streams pass different ``workspace_slot``s."""
+    different streams pass different ``workspace_slot``s.  With ``status`` (a DeviceStatus
+    the caller checks later) the call neither allocates a status word nor synchronises, so
+    it can be captured into a CUDA graph once its workspace slot is large enough."""
     lib = nat.load_library()
     n_block, n_energy, n, _ = Y.shape
     n_sector = half_steps.numel()
     is_complex = int(Y.is_complex())
     dev = Y.device
+    check_now = status is None
     with torch.cuda.device(dev):
-        nbytes = nat.size_query(lib.ticc_ldmd_blocks_workspace_size, n, n_energy, n_block, n_sector, is_complex, precision)
+        nbytes = blocks_workspace_bytes(n, n_energy, n_block, n_sector, bool(is_complex), precision)
         work = nat.Workspace.get(dev, nbytes, slot=workspace_slot)
-        status = nat.DeviceStatus(dev)
+        status = nat.DeviceStatus(dev) if status is None else status
         nat.check(
             lib.ticc_ldmd_propagate_blocks(
                 nat.ptr(Y), is_complex, nat.ptr(energies), n_energy, float(reduced_mass), nat.ptr(half_steps),
@@ -116,7 +123,8 @@ def propagate_blocks_device(Y: torch.Tensor, energies: torch.Tensor, reduced_mas
             ),
             "ticc_ldmd_propagate_blocks",
         )
-        status.raise_if_failed("ticc_ldmd_propagate_blocks")
+        if check_now:
+            status.raise_if_failed("ticc_ldmd_propagate_blocks")
     return Y
 
 

@@ -185,22 +185,29 @@ CLASS_WORKSPACE_SLOT = 16  # first workspace slot of the concurrently propagated
 
 
 class DeviceBlocks:
-    """Device-resident pieces of several channel blocks of one Hamiltonian, padded to the
-    largest block size n: per block its rows (output positions inside the block), its
-    centrifugal matrix U and thresholds E_int.  Padding channels have no coupling, U = 0
+    """Device-resident pieces of several channel blocks, padded to the largest block size n:
+    per block its rows (output positions inside the block), its centrifugal matrix U and
+    thresholds E_int.  ``entries`` lists (hamiltonian, channel indices) pairs: the K blocks of
+    one Hamiltonian (coupled states, NNCC) or whole systems of a partial-wave sweep, which
+    must share one PotentialGrid and reduced mass.  Padding channels have no coupling, U = 0
     and a threshold set per call far above the highest energy, so they stay closed and
     decoupled.  With ``closed_first`` each block's channels are ordered most-closed first
     (by W_ii at the outermost grid point), as for one exact-CC block."""
 
-    def __init__(self, hamiltonian, blocks: tuple[tuple[int, ...], ...], device: torch.device, closed_first: bool = False) -> None:
-        self.grid = hamiltonian.potential_grid
+    def __init__(self, entries, device: torch.device, closed_first: bool = False) -> None:
+        first = entries[0][0]
+        self.grid = first.potential_grid
         self.values = self.grid.device_values(device)
-        self.reduced_mass = hamiltonian.reduced_mass
-        self.sizes = tuple(len(b) for b in blocks)
+        self.reduced_mass = first.reduced_mass
+        if any(h.potential_grid is not self.grid or h.reduced_mass != self.reduced_mass for h, _ in entries):
+            message = "Blocks propagated together must share one PotentialGrid and reduced mass"
+            logger.error(message)
+            raise ValueError(message)
+        self.sizes = tuple(len(b) for _, b in entries)
         self.n = max(self.sizes)
         self.rows, self.U, self.E_int, self.position = [], [], [], []
         outer = self.grid.radial_points[-1:]
-        for block in blocks:
+        for hamiltonian, block in entries:
             indices = np.asarray(block, dtype=np.int64)
             U = np.asarray(hamiltonian.centrifugal(block))
             E_int = np.asarray(hamiltonian.E_int)[indices]
@@ -242,7 +249,7 @@ class DeviceBlocks:
 
 
 def device_blocks(hamiltonian, blocks, device: torch.device, closed_first: bool = False) -> DeviceBlocks:
-    return _device_state(hamiltonian, ("blocks", blocks, device.index, closed_first), lambda: DeviceBlocks(hamiltonian, blocks, device, closed_first))
+    return _device_state(hamiltonian, ("blocks", blocks, device.index, closed_first), lambda: DeviceBlocks([(hamiltonian, b) for b in blocks], device, closed_first))
 
 
 def blocks_window(n_channel: int, n_block: int, n_sector: int) -> int:
