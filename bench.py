@@ -360,10 +360,10 @@ def main():
     # every headline S against the plain FP64 S of the same unit, and its unitarity defect
     per_S_dS, per_S_unitarity, counts_equal = [], [], True
     for k, ((S_h, n_h), out_p) in enumerate(zip(head_out, plain_out + [None] * (len(head_out) - len(plain_out)))):
-        n_h = n_h.cpu().numpy()
+        n_h = np.asarray(n_h)
         S_h = S_h.cpu().numpy()
         if out_p is not None:
-            S_p, n_p = out_p[0].cpu().numpy(), out_p[1].cpu().numpy()
+            S_p, n_p = out_p[0].cpu().numpy(), np.asarray(out_p[1])
             counts_equal &= bool(np.array_equal(n_h, n_p))
         for e, m in enumerate(n_h):
             s = S_h[e, :m, :m]
@@ -380,7 +380,7 @@ def main():
             idx = np.asarray(fixture["energy_indices"])
             for name, config in (("headline", headline), ("plain_fp64", plain)):
                 S, n_open = one_step(b, idx, config)
-                S, n_open = S.cpu().numpy(), n_open.cpu().numpy()
+                S, n_open = S.cpu().numpy(), np.asarray(n_open)
                 worst = max(float(np.abs(S[e, :m, :m] - fixture["Smat"][e, :m, :m]).max()) for e, m in enumerate(n_open) if m)
                 entry = ref.setdefault(name, {"max_dS": 0.0, "open_counts_equal": True, "fixtures": []})
                 entry["max_dS"] = max(entry["max_dS"], worst)

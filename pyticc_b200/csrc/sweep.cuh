@@ -733,6 +733,10 @@ __device__ inline void update_unit_split(double* Mb, int ld, int k0, int r0, int
 // sits after both.
 constexpr size_t kStepSlotOffset = (size_t(kTcSmemBytes) > kUpdTileSmemBytes ? size_t(kTcSmemBytes) : kUpdTileSmemBytes);
 constexpr size_t kStepSmemBytes = kStepSlotOffset + 16;
+// The FP64 units (row panels, pivots, mma.sync updates) that share a CTA with the tcgen05
+// units overwrite shared memory below kUpdTileSmemBytes between them: the tcgen05 barriers
+// and TMEM slot, which live across units, must sit above it.
+static_assert(size_t(kTcBarOffset) >= kUpdTileSmemBytes, "tcgen05 barriers must lie beyond the FP64 units' shared memory");
 
 // In a reduced step with `split` (and tensor maps over it and M), the trailing-update tiles
 // run on the tcgen05 tensor core (tc_update_unit); otherwise on the mma.sync paths.
@@ -815,6 +819,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1) sweep_step_kernel(double* __r
     double* Mb = M + (long long)b * mstride;
     const double* Cb = cold + (long long)b * cstride;
     if (tensor_core) {
+      // units come in queue order (row panels, pivots, then updates), so no unit that
+      // overwrites shared memory follows a tcgen05 unit whose C store may still be reading it;
       // after a failed unit this CTA's tensor-core state is unknown: it only drains the queue
       if (tc_live && !tc_update_unit(tcs, maps, b, ta, tb, abort_flag, status)) tc_live = false;
     } else if (reduced) {

@@ -87,14 +87,27 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
 __device__ __forceinline__ void fence_proxy_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
 
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
-  asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
-               "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+// L2 policies: the split operand panels are re-read by every tile of their row or column
+// (keep them), the FP64 C tiles pass through once (let them go first).
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar, uint64_t policy) {
+  asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%2, %3, %4}], [%5], %6;" ::"r"(dst),
+               "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar), "l"(policy)
                : "memory");
 }
-__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, uint32_t src, int x, int y, int z) {
-  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(reinterpret_cast<uint64_t>(map)), "r"(src), "r"(x), "r"(y),
-               "r"(z)
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, uint32_t src, int x, int y, int z, uint64_t policy) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group.L2::cache_hint [%0, {%2, %3, %4}], [%1], %5;" ::"l"(reinterpret_cast<uint64_t>(map)), "r"(src),
+               "r"(x), "r"(y), "r"(z), "l"(policy)
                : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
@@ -212,10 +225,11 @@ __device__ __forceinline__ void tc_issue_chunk(const TcState& s, const CUtensorM
   const uint32_t full = tc_bar(s, kTcFull + stage);
   mbar_expect_tx(full, kTcStageBytes);
   const int nt = s.nt;
-  tma_load_3d(dst + 0 * kTcArrayBytes, split, 0, 0, tc_split_block(b, 0, nt, ta, c), full);
-  tma_load_3d(dst + 1 * kTcArrayBytes, split, 0, 0, tc_split_block(b, 1, nt, ta, c), full);
-  tma_load_3d(dst + 2 * kTcArrayBytes, split, 0, 0, tc_split_block(b, 2, nt, tb, c), full);
-  tma_load_3d(dst + 3 * kTcArrayBytes, split, 0, 0, tc_split_block(b, 3, nt, tb, c), full);
+  const uint64_t keep = l2_policy_evict_last();
+  tma_load_3d(dst + 0 * kTcArrayBytes, split, 0, 0, tc_split_block(b, 0, nt, ta, c), full, keep);
+  tma_load_3d(dst + 1 * kTcArrayBytes, split, 0, 0, tc_split_block(b, 1, nt, ta, c), full, keep);
+  tma_load_3d(dst + 2 * kTcArrayBytes, split, 0, 0, tc_split_block(b, 2, nt, tb, c), full, keep);
+  tma_load_3d(dst + 3 * kTcArrayBytes, split, 0, 0, tc_split_block(b, 3, nt, tb, c), full, keep);
 }
 
 // One update tile.  Returns false (on every thread) if a wait gave up; the abort flag and
@@ -230,16 +244,11 @@ __device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int
     unsigned loads_pending = 0;  // stages whose TMA load was issued and not yet waited
     uint32_t pending_parity[kTcStages] = {};
     bool c_pending = false, mma_issued = false;
-    // the C tile: the previous unit's generic accesses of the buffer are ordered before this
-    // load by the barrier that ended it and this proxy fence; split panels written by other
-    // CTAs of this launch were released to this thread by the flag it acquired
+    // split panels written by other CTAs of this launch were released to this thread by the
+    // flag it acquired; the stages were last read by the previous unit's MMAs (waited for)
     fence_proxy_async_shared();
     fence_proxy_async_global();
-    const uint32_t cbar = tc_bar(s, kTcCFull);
-    mbar_expect_tx(cbar, kTcCBytes);
-    for (int q = 0; q < 8; ++q) tma_load_3d(s.base_u + (uint32_t)q * kTcCChunkBytes, &maps.matrix, c0 + 16 * q, r0, b, cbar);
-    c_pending = true;
-    // operand ring: chunk g = s.chunk + c uses stage g % kTcStages in its (g / kTcStages)-th use
+    // operand ring first: chunk g = s.chunk + c uses stage g % kTcStages in its (g / kTcStages)-th use
     const uint32_t g0 = s.chunk;
     auto issue = [&](int c, uint32_t g) {
       const int stage = g % kTcStages;
@@ -252,6 +261,17 @@ __device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int
       // the MMAs that last read this stage (chunk g - kTcStages) have completed
       if (g >= (uint32_t)kTcStages && !mbar_wait(tc_bar(s, kTcEmpty + g % kTcStages), ((g - kTcStages) / kTcStages) & 1u)) ok = 0;
       if (ok) issue(c, g);
+    }
+    // then the C tile, once the previous unit's TMA store has read the buffer out (its
+    // generic writes were ordered before that store by a proxy fence and a barrier)
+    const uint32_t cbar = tc_bar(s, kTcCFull);
+    if (ok) {
+      bulk_wait_read_all();
+      fence_proxy_async_shared();
+      mbar_expect_tx(cbar, kTcCBytes);
+      const uint64_t once = l2_policy_evict_first();
+      for (int q = 0; q < 8; ++q) tma_load_3d(s.base_u + (uint32_t)q * kTcCChunkBytes, &maps.matrix, c0 + 16 * q, r0, b, cbar, once);
+      c_pending = true;
     }
     tc_fence_after();
     for (int c = 0; c < nchunks && ok; ++c) {
@@ -340,9 +360,10 @@ __device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int
   fence_proxy_async_shared();
   __syncthreads();
   if (tid == 0) {
-    for (int q = 0; q < 8; ++q) tma_store_3d(&maps.matrix, s.base_u + (uint32_t)q * kTcCChunkBytes, c0 + 16 * q, r0, b);
+    // the next unit waits for this store to have read the buffer before it reloads C
+    const uint64_t once = l2_policy_evict_first();
+    for (int q = 0; q < 8; ++q) tma_store_3d(&maps.matrix, s.base_u + (uint32_t)q * kTcCChunkBytes, c0 + 16 * q, r0, b, once);
     bulk_commit();
-    bulk_wait_read_all();  // the C buffer is reused by the next unit's load
   }
   ++s.tile;
   __syncthreads();
