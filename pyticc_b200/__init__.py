@@ -12,7 +12,7 @@ from .cross_section import PartialCrossSections, partial_cross_sections
 from .energy import get_Etot
 from .match import get_Bmat_BF_to_SF, get_Smat, modified_bessel_K_logD, riccati_bessel_jy, transform_logD_BF_to_SF
 from .pes import PESWrapper
-from .propagation import Propagation, build_radial_sectors, propagate_logD
+from .propagation import PartialWaveSweep, Propagation, build_radial_sectors, propagate_logD, solve_sweep
 from .kblock import KBlock, build_cs_blocks, build_nncc_blocks
 from .result import CoupledStatesResult, KBlockResult, ScatteringResult, Timing
 from .scattering import PotentialGrid, ScattHamiltonian, build_k_blocks, finalize_K_block, prepare_potential, solve
@@ -21,10 +21,10 @@ from .system import Approx, ChannelSpec, ScatteringType, ScattSystem, build_Scat
 __all__ = [
     "AMU2AU", "AU2CM", "AU2K", "CM2AU", "K2AU",
     "Approx", "AtomSpec", "Channel", "ChannelBasis", "ChannelSpec", "CoupledStatesResult", "DiatomBasis", "DiatomSpec", "KBlock", "KBlockResult",
-    "PESWrapper", "PartialCrossSections", "PotentialGrid",
+    "PESWrapper", "PartialCrossSections", "PartialWaveSweep", "PotentialGrid",
     "Propagation", "RovibBasis", "ScattHamiltonian", "ScattSystem", "ScatteringResult", "ScatteringType", "Timing",
     "build_ChannelBasis", "build_RovibDVR", "build_ScattSystem", "build_SineDVR", "build_cs_blocks", "build_k_blocks", "build_nncc_blocks",
     "build_radial_sectors", "finalize_K_block", "get_Bmat_BF_to_SF",
     "get_Etot", "get_Smat", "get_Umat_BF", "modified_bessel_K_logD", "partial_cross_sections", "prepare_potential", "propagate_logD", "reduced_mass",
-    "riccati_bessel_jy", "solve", "transform_logD_BF_to_SF",
+    "riccati_bessel_jy", "solve", "solve_sweep", "transform_logD_BF_to_SF",
 ]

@@ -4,8 +4,10 @@ from .config import Propagation, PropagationMode, resolve_device
 from .grid import RadialSector, build_radial_sectors, iter_radial_windows
 from .logd import initialize_logD_capture, initialize_logD_inelastic, propagate_logD, propagate_logD_sector
 from .runner import propagate, propagate_blocks
+from .sweep import PartialWaveSweep, solve_sweep
 
 __all__ = [
+    "PartialWaveSweep",
     "Propagation",
     "PropagationMode",
     "RadialSector",
@@ -18,4 +20,5 @@ __all__ = [
     "propagate_logD",
     "propagate_logD_sector",
     "resolve_device",
+    "solve_sweep",
 ]

@@ -10,6 +10,7 @@ Y stays on the device for the whole traversal.  Windows are sized by device memo
 from __future__ import annotations
 
 from collections.abc import Sequence
+from copy import copy
 from concurrent.futures import ThreadPoolExecutor
 from math import ceil
 from time import perf_counter
@@ -184,48 +185,72 @@ DUMMY_P2 = 3600.0  # local wavenumber^2 (bohr^-2) of the closed channels that pa
 CLASS_WORKSPACE_SLOT = 16  # first workspace slot of the concurrently propagated size classes
 
 
+class BlockState:
+    """One channel block on a device, built once: rows (output positions inside the block),
+    centrifugal matrix U and thresholds E_int in propagation order, and ``position`` (the
+    propagated index of each block channel).  With ``closed_first`` the order is most-closed
+    first (by W_ii at the outermost grid point), as for one exact-CC block."""
+
+    def __init__(self, hamiltonian, block: tuple[int, ...], device: torch.device, closed_first: bool = False) -> None:
+        grid = hamiltonian.potential_grid
+        indices = np.asarray(block, dtype=np.int64)
+        U = np.asarray(hamiltonian.centrifugal(block))
+        E_int = np.asarray(hamiltonian.E_int)[indices]
+        order = np.arange(indices.size)
+        if closed_first:
+            rows = device_rows(hamiltonian.V_basis, device, block)
+            outer = grid.radial_points[-1:]
+            index = torch.as_tensor(grid.selection(outer), device=device)
+            W = contract_rows(rows, grid.device_values(device).index_select(0, index), radial_points=torch.as_tensor(outer, device=device),
+                              U=torch.as_tensor(U, device=device), E_int=torch.as_tensor(E_int, device=device), reduced_mass=hamiltonian.reduced_mass)[0]
+            order = np.argsort(-torch.diagonal(W).cpu().numpy(), kind="stable")
+        self.hamiltonian = hamiltonian
+        self.size = int(indices.size)
+        self.rows = device_rows(hamiltonian.V_basis, device, tuple(int(c) for c in indices[order]))
+        self.U = U[np.ix_(order, order)]
+        self.E_int = E_int[order]
+        position = np.empty_like(order)
+        position[order] = np.arange(order.size)
+        self.position = torch.as_tensor(position, device=device)
+
+
 class DeviceBlocks:
     """Device-resident pieces of several channel blocks, padded to the largest block size n:
     per block its rows (output positions inside the block), its centrifugal matrix U and
     thresholds E_int.  ``entries`` lists (hamiltonian, channel indices) pairs: the K blocks of
     one Hamiltonian (coupled states, NNCC) or whole systems of a partial-wave sweep, which
-    must share one PotentialGrid and reduced mass.  Padding channels have no coupling, U = 0
+    must share one PotentialGrid and reduced mass (or ``states``: prebuilt BlockStates, and
+    ``n``: a padded size at least their largest).  Padding channels have no coupling, U = 0
     and a threshold set per call far above the highest energy, so they stay closed and
-    decoupled.  With ``closed_first`` each block's channels are ordered most-closed first
-    (by W_ii at the outermost grid point), as for one exact-CC block."""
+    decoupled.  With ``closed_first`` each block's channels are ordered most-closed first."""
 
-    def __init__(self, entries, device: torch.device, closed_first: bool = False) -> None:
-        first = entries[0][0]
+    def __init__(self, entries, device: torch.device, closed_first: bool = False, *, states=None, n: int | None = None) -> None:
+        if states is None:
+            states = [BlockState(h, tuple(b), device, closed_first) for h, b in entries]
+        first = states[0].hamiltonian
         self.grid = first.potential_grid
         self.values = self.grid.device_values(device)
         self.reduced_mass = first.reduced_mass
-        if any(h.potential_grid is not self.grid or h.reduced_mass != self.reduced_mass for h, _ in entries):
+        if any(st.hamiltonian.potential_grid is not self.grid or st.hamiltonian.reduced_mass != self.reduced_mass for st in states):
             message = "Blocks propagated together must share one PotentialGrid and reduced mass"
             logger.error(message)
             raise ValueError(message)
-        self.sizes = tuple(len(b) for _, b in entries)
-        self.n = max(self.sizes)
+        self.sizes = tuple(st.size for st in states)
+        self.n = max(self.sizes) if n is None else int(n)
+        if self.n < max(self.sizes):
+            message = f"Padded block size {self.n} is below the largest block ({max(self.sizes)} channels)"
+            logger.error(message)
+            raise ValueError(message)
         self.rows, self.U, self.E_int, self.position = [], [], [], []
-        outer = self.grid.radial_points[-1:]
-        for hamiltonian, block in entries:
-            indices = np.asarray(block, dtype=np.int64)
-            U = np.asarray(hamiltonian.centrifugal(block))
-            E_int = np.asarray(hamiltonian.E_int)[indices]
-            order = np.arange(indices.size)
-            if closed_first:
-                rows = device_rows(hamiltonian.V_basis, device, block)
-                W = self._contract(rows, outer, torch.as_tensor(U, device=device), torch.as_tensor(E_int, device=device))[0]
-                order = np.argsort(-torch.diagonal(W).cpu().numpy(), kind="stable")
-            rows = device_rows(hamiltonian.V_basis, device, tuple(int(c) for c in indices[order]))
+        for st in states:
+            rows = copy(st.rows)
             rows.n_channel = self.n
             U_pad = np.zeros((self.n, self.n))
-            U_pad[: order.size, : order.size] = U[np.ix_(order, order)]
-            position = np.empty_like(order)
-            position[order] = np.arange(order.size)
+            U_pad[: st.size, : st.size] = st.U
             self.rows.append(rows)
             self.U.append(torch.as_tensor(U_pad, device=device))
-            self.E_int.append(E_int[order])
-            self.position.append(torch.as_tensor(position, device=device))
+            self.E_int.append(st.E_int)
+            self.position.append(st.position)
 
     def _contract(self, rows, radial_points, U, E_int, out=None):
         dev = U.device

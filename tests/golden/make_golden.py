@@ -605,9 +605,16 @@ def make_full_morse() -> None:
 
 
 def make_full_capture() -> None:
-    """The ultracold capture block at full size: rigid rotor B=0.03 cm^-1, j<=40, J=10 (N=396),
+    """The ultracold capture block at full size: rigid rotor B=0.03 cm^-1, j<=40, J=10 (N=396;
+    optional other J values after the name: ``make_golden.py <src> full_capture 0 1``),
     capture boundary at 8 bohr, fixed step h=0.05 to 1500 bohr, at 1 uK and 1 mK."""
-    params = {"B_cm": 0.03, "jmax": 40, "J": 10, "parity": 1, "mu_amu": 100.0, "C6": 1.0e4, "wall_cm": 500.0, "seed": 3, "n_theta": 48, "boundaries": [8.0, 1500.0], "half_steps": [0.05], "energies_K": [1.0e-6, 1.0e-3]}
+    J_values = [int(v) for v in sys.argv[3:]] if len(sys.argv) > 3 and sys.argv[2] == "full_capture" else [10]
+    for J in J_values:
+        _make_full_capture(J)
+
+
+def _make_full_capture(J: int) -> None:
+    params = {"B_cm": 0.03, "jmax": 40, "J": J, "parity": 1, "mu_amu": 100.0, "C6": 1.0e4, "wall_cm": 500.0, "seed": 3, "n_theta": 48, "boundaries": [8.0, 1500.0], "half_steps": [0.05], "energies_K": [1.0e-6, 1.0e-3]}
     g = np.random.default_rng(params["seed"]).uniform(0.2, 1.0, size=3)
 
     def interaction(R, coordinates):
@@ -626,7 +633,7 @@ def make_full_capture() -> None:
         reduced_mass=params["mu_amu"] * AMU,
     )
     energies = np.asarray(params["energies_K"]) * K2AU
-    _solve_full_and_save("full_capture_J10", params, system, params["boundaries"], params["half_steps"], energies, "capture", n_theta=params["n_theta"])
+    _solve_full_and_save(f"full_capture_J{J}", params, system, params["boundaries"], params["half_steps"], energies, "capture", n_theta=params["n_theta"])
 
 
 def make_dropin() -> None:
@@ -704,7 +711,7 @@ FULL_SIZE_MAKERS = {
 if __name__ == "__main__":
     # python make_golden.py <reference src> [fixture names...]  (default: all small fixtures)
     names = sys.argv[2:] or list(MAKERS)
-    if names and names[0] == "full_morse":
-        names = ["full_morse"]
+    if names and names[0] in ("full_morse", "full_capture"):
+        names = names[:1]
     for key in names:
         {**MAKERS, **FULL_SIZE_MAKERS}[key]()
