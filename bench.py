@@ -45,6 +45,9 @@ def parse_args():
     p.add_argument("--plain-steps", type=int, default=None, help="timed steps of the plain FP64 fixed-step arm (default: steps - 1, at least 1)")
     p.add_argument("--sectors", type=int, default=0, help="limit sectors (0 = all 938); for quick checks only")
     p.add_argument("--approx", choices=["exact", "cs", "nncc"], default="exact", help="exact CC (the metric) or the coupled-states / NNCC (K_delta=1) blocks of the same system")
+    p.add_argument("--config", choices=["vibrating", "sweep", "capture"], default="vibrating",
+                   help="vibrating: the headline J=30 blocks; sweep: the batched partial-wave sweep of the same system; capture: the ultracold capture system with learned widths")
+    p.add_argument("--sweep-J-step", type=int, default=12, help="sweep: every n-th J of 0..60 (1 = all 61)")
     return p.parse_args()
 
 
@@ -275,6 +278,12 @@ def main():
     if args.approx != "exact":
         run_blocks(args, rank, world, local)
         return
+    if args.config == "sweep":
+        run_sweep(args, rank, world, local)
+        return
+    if args.config == "capture":
+        run_capture(args, rank, world, local)
+        return
     import torch
 
     import pyticc_b200 as tb
@@ -477,6 +486,172 @@ def main():
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _timed_loop(torch, fn, steps):
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    outs = [fn(k) for k in range(steps)]
+    stop.record()
+    torch.cuda.synchronize()
+    return start.elapsed_time(stop) * 1e-3, outs
+
+
+def run_sweep(args, rank, world, local):
+    """The batched partial-wave sweep of the vibrating A+BC system: J = 0..60 (every
+    --sweep-J-step-th), both parities, 64 energies log-uniform over 1-3000 cm^-1 per block,
+    --batch of them per step (one step = every block at one energy batch); all blocks in one
+    CUDA graph (first run direct, then replays).  Headline: mixed precision; then plain FP64."""
+    import torch
+
+    import pyticc_b200 as tb
+    from pyticc_b200 import _native as nat
+    from pyticc_b200 import workloads
+    from pyticc_b200.replicas import max_over_ranks
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = nat.load_library()
+    diatom = workloads.morse_diatom(**workloads.MORSE_DEFAULTS)
+    base = workloads.morse_atom_diatom(parity=1, diatom=diatom, n_energy=1)
+    Js = list(range(0, 61, max(1, args.sweep_J_step)))
+    pes = base.system.potential
+    systems = [tb.build_ScattSystem(tb.AtomSpec(), diatom, Jtot=J, system_parity=p, potential=pes, reduced_mass=base.system.reduced_mass) for J in Js for p in (1, -1)]
+    energies_all = np.geomspace(1.0, 3000.0, 64) * tb.CM2AU
+    batch = min(args.batch, 64)
+    batches = [energies_all[(np.arange(batch) * (64 // batch) + k) % 64] for k in range(64 // batch)]
+    sizes = [s.basis.n_channel for s in systems]
+    flops_per_energy = sum(2.0 * n**3 for n in sizes) * len(base.grid.sectors)
+    from pyticc_b200.match.asymptotic import get_Bmat_BF_to_SF
+    from pyticc_b200.scattering import _match
+
+    BL = [get_Bmat_BF_to_SF(s.basis) if s.basis.n_channel else None for s in systems]
+    Rmatch = base.grid.sectors[-1].radial_end
+
+    def matched(Ys, E):
+        return [None if Y is None else _match(Y, BL[i][0], BL[i][1], systems[i].basis.E_int, Rmatch, E, float(systems[i].reduced_mass)) for i, Y in enumerate(Ys)]
+
+    arms = {}
+    for precision in ("mixed", "fp64"):
+        config = tb.Propagation(precision=precision)
+        sweep = tb.PartialWaveSweep(systems, base.grid, config, n_energy=batch, energy_bound=float(energies_all.max()), graph=True)
+        for k in range(args.warmup):
+            sweep.propagate(batches[k % len(batches)])  # the first run also captures the graph
+        launches0 = lib.ticc_kernel_launches()
+
+        def step(k, sweep=sweep):
+            E = batches[(args.warmup + k) % len(batches)]
+            return matched(sweep.propagate(E), E)
+
+        with ClockSampler(local) as clocks:
+            elapsed, outs = _timed_loop(torch, step, args.steps)
+        elapsed = max_over_ranks(elapsed, None)
+        # kernels inside graph replays do not pass the library's launch counter: add the
+        # captured launches once per replay
+        launches = lib.ticc_kernel_launches() - launches0 + args.steps * sweep.graph_launches
+        arms[precision] = {"seconds": elapsed, "launches": launches, "clocks": clocks.summary(), "S": outs[0], "sweep": sweep}
+    n_solves = sum(1 for n in sizes if n) * batch * args.steps
+    head, plain = arms["mixed"], arms["fp64"]
+    value = n_solves / head["seconds"]
+    plain_value = n_solves / plain["seconds"]
+    # accuracy: the first timed batch in both arms, every S
+    worst, defect = 0.0, 0.0
+    for Sh, Sp in zip(head["S"], plain["S"], strict=True):
+        if Sh is None:
+            continue
+        for a, b in zip(Sh, Sp, strict=True):
+            if a.size:
+                worst = max(worst, float(np.abs(a - b).max()))
+                defect = max(defect, float(np.abs(a.conj().T @ a - np.eye(a.shape[0])).max()))
+    peak = _best_gemm_tflops(torch, dev, torch.float64)
+    achieved = flops_per_energy * batch * args.steps / head["seconds"] / 1e12
+    plain_achieved = flops_per_energy * batch * args.steps / plain["seconds"] / 1e12
+    line = {
+        "metric": "S-matrix solves/s on 1 B200, batched partial-wave sweep (one solve = one (J, parity) block at one energy)",
+        "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": head["seconds"] / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64+tf32x3", "data": "synthetic",
+        "config": {"workload": f"vibrating A+BC sweep: Morse diatom v<=3 j<=30, J in {Js[0]}..{Js[-1]} step {Js[1] - Js[0] if len(Js) > 1 else 1}, both parities ({len(systems)} blocks, {sum(1 for n in sizes if not n)} empty, N {min(n for n in sizes if n)}-{max(sizes)}), 938 sectors, 64 energies log-uniform 1-3000 cm^-1",
+                   "batch": batch, "launches": len(head["sweep"].launches), "classes_merged": sorted(k for k, v in head["sweep"].merges.items() if v), "graph": True,
+                   "l2": "inputs larger than L2 (work matrices of the large blocks 32 MiB each per energy)"},
+        "plain_fp64": {"value": plain_value, "ms_per_step": plain["seconds"] / args.steps * 1e3, "speedup_of_value": value / plain_value,
+                       "roofline": {"bound": "tensor", "achieved": plain_achieved, "peak": peak, "unit": "TFLOP/s", "frac": plain_achieved / peak}},
+        "accuracy": {"max_dS_vs_plain_fp64": worst, "unitarity_defect_max": defect, "tolerance": 1e-6, "energies": batch},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "peak_note": "cuBLAS DGEMM measured in this run; flops are FP64-equivalent (sum over blocks of 2 N^3 per (sector, energy))"},
+        "e2e": None,
+        "gpu_launches": int(head["launches"]),
+        "clocks": head["clocks"],
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_capture(args, rank, world, local):
+    """The ultracold capture system (rigid rotor B=0.03 cm^-1, j<=40, capture boundary at 8
+    bohr, fixed step h=0.05 to 1500 bohr) at J = 0, 5, 10 with energies log-uniform over
+    1 uK-1 mK, --batch per step: learned sector widths (judged inside solve) against the fixed
+    grid, both timed; accuracy against the reference's full-size S at J = 0 and J = 10."""
+    import torch
+
+    import pyticc_b200 as tb
+    from pyticc_b200 import _native as nat
+    from pyticc_b200 import workloads
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = nat.load_library()
+    Js = (0, 5, 10)
+    blocks = [workloads.ultracold_capture(J=J, n_energy=512) for J in Js]
+    batch = min(args.batch, 512)
+    arms = {}
+    span = (min(float(wl.energies.min()) for wl in blocks), max(float(wl.energies.max()) for wl in blocks))
+    for steps_kind in ("learned", "fixed"):
+        # the learned schedule is built and judged once for the whole energy range
+        config = tb.Propagation(mode="capture", precision="mixed", steps=steps_kind, learned_range=span if steps_kind == "learned" else None)
+        used: list = []
+
+        def step(k, config=config, used=used):
+            out = []
+            for wl in blocks:
+                E = wl.energies[(np.arange(batch) * (512 // batch) + k) % 512]
+                stats: dict = {}
+                out.append(tb.solve(wl.system, E, wl.grid, config, stats=stats))
+                used.append(stats.get("sectors"))
+            return out
+
+        for k in range(args.warmup):
+            step(k)
+        used.clear()
+        launches0 = lib.ticc_kernel_launches()
+        with ClockSampler(local) as clocks:
+            elapsed, _ = _timed_loop(torch, lambda k: step(args.warmup + k), args.steps)
+        arms[steps_kind] = {"seconds": elapsed, "sectors": list(used), "launches": lib.ticc_kernel_launches() - launches0, "clocks": clocks.summary()}
+    accuracy = {}
+    for J, name in ((0, "full_capture_J0.npz"), (10, "full_capture_J10.npz")):
+        path = ROOT / "tests" / "golden" / name
+        if not path.exists():
+            continue
+        data = np.load(path)
+        wl = blocks[Js.index(J)]
+        result = tb.solve(wl.system, data["energies"], wl.grid, tb.Propagation(mode="capture", precision="mixed", steps="learned", learned_range=span))
+        accuracy[f"J{J}"] = max((float(np.abs(s - data["Smat"][e, : s.shape[0], : s.shape[0]]).max()) for e, s in enumerate(result.Smat) if s.size), default=0.0)
+    n_solves = len(blocks) * batch * args.steps
+    head, fixed = arms["learned"], arms["fixed"]
+    line = {
+        "metric": "S-matrix solves/s on 1 B200, ultracold capture with learned sector widths (one solve = one (J, parity) block at one energy)",
+        "value": n_solves / head["seconds"], "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": head["seconds"] / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c128 via real embedding, f64+tf32x3", "data": "synthetic",
+        "config": {"workload": "ultracold capture: rigid rotor B=0.03 cm^-1 j<=40, J=0,5,10 parity +1 (N=41..396 complex), C6 tail + Gaussian wall, capture boundary 8 bohr, fixed h=0.05 to 1500 bohr (14920 sectors), 512 energies log-uniform 1 uK-1 mK",
+                   "batch": batch, "sectors_fixed": len(blocks[0].grid.sectors), "sectors_learned_per_block": head["sectors"][: len(blocks)]},
+        "fixed_grid": {"value": n_solves / fixed["seconds"], "ms_per_step": fixed["seconds"] / args.steps * 1e3, "speedup_of_learned": fixed["seconds"] / head["seconds"]},
+        "accuracy": {"max_dS_vs_reference_fixed_step": accuracy, "tolerance": 1e-6},
+        "e2e": None,
+        "gpu_launches": int(head["launches"]),
+        "clocks": head["clocks"],
     }
     print(json.dumps(line), flush=True)
 

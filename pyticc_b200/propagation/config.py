@@ -51,6 +51,9 @@ class Propagation:
     proposed by ``proposer``, a StepProposer or a path to its weights; None = the
     packaged default), used only once a fixed-step solve at the lowest and highest energy
     of the call agrees with it within ``judge_tol`` (max|dS|, equal open counts);
+    learned_range: (E_min, E_max) in hartree the learned schedule is built and judged for;
+    every call whose energies lie inside reuses that one schedule and its cached verdict
+    (without it each call's own lowest and highest energy define the schedule);
     audit: also solve every energy in plain FP64 with fixed steps and attach max|dS| per
     energy to the result (doubles the cost; for validation runs)."""
 
@@ -62,6 +65,7 @@ class Propagation:
     steps: str = "fixed"
     proposer: object = None
     judge_tol: float = 1.0e-6
+    learned_range: tuple | None = None
     audit: bool = False
 
     def __post_init__(self) -> None:
@@ -90,6 +94,13 @@ class Propagation:
             message = f"Propagation judge_tol must be positive, but got {self.judge_tol}"
             logger.error(message)
             raise ValueError(message)
+        if self.learned_range is not None:
+            lo, hi = (float(v) for v in self.learned_range)
+            if not (np.isfinite(lo) and np.isfinite(hi) and lo <= hi):
+                message = f"Propagation learned_range must be (E_min, E_max) with E_min <= E_max, but got {self.learned_range!r}"
+                logger.error(message)
+                raise ValueError(message)
+            object.__setattr__(self, "learned_range", (lo, hi))
         if not isinstance(self.audit, bool):
             message = f"Propagation audit must be a boolean, but got {self.audit!r}"
             logger.error(message)

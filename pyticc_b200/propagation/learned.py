@@ -353,26 +353,43 @@ def learned_sectors(hamiltonian, sectors: Sequence[RadialSector], Etot, proposer
 
 def judged_learned_sectors(problem, potential_grid, Etot, propagation: Propagation) -> tuple[tuple[RadialSector, ...], dict]:
     """The learned schedule for these energies if the fixed step accepts it, else the fixed
-    grid.  The judge solves the lowest and the highest energy of the call with both
-    schedules (same precision and mode) and accepts when the open counts are equal and
-    max|dS| <= ``propagation.judge_tol``.  Verdicts are cached per schedule on the
-    Hamiltonian, so repeated calls with the same schedule are judged once; a schedule equal
-    to the fixed grid needs no judge.  Returns (sectors, record) with record holding the
+    grid.  The schedule is built for the call's lowest and highest energy, or for
+    ``propagation.learned_range`` (then built once and cached); the judge solves those two
+    energies with both schedules (same precision and mode) and accepts when the open counts
+    are equal and max|dS| <= ``propagation.judge_tol``.  Verdicts are cached per schedule on
+    the Hamiltonian, so repeated calls with the same schedule are judged once; a schedule
+    equal to the fixed grid needs no judge.  Returns (sectors, record) with record holding the
     decision, max|dS| of the judge and both sector counts."""
     from ..scattering import hamiltonian_for, solve
 
     hamiltonian = hamiltonian_for(problem, potential_grid)
     fixed = tuple(potential_grid.sectors)
     energies = np.atleast_1d(np.asarray(Etot, dtype=np.float64))
-    schedule = learned_sectors(hamiltonian, fixed, energies, resolve_proposer(propagation.proposer), propagation.device)
+    cache = getattr(hamiltonian, "_runner_cache", {})
+    span = (float(energies.min()), float(energies.max()))
+    if propagation.learned_range is not None:
+        lo, hi = propagation.learned_range
+        if span[0] < lo or span[1] > hi:
+            message = f"Energies {span} lie outside the learned_range {propagation.learned_range}"
+            logger.error(message)
+            raise ValueError(message)
+        span = (lo, hi)
+    proposer = resolve_proposer(propagation.proposer)
+    schedule_key = ("learned_schedule", span, len(fixed))
+    cached = cache.get(schedule_key)
+    if cached is not None and cached[0] is proposer:
+        schedule = cached[1]
+    else:
+        schedule = learned_sectors(hamiltonian, fixed, np.asarray(span), proposer, propagation.device)
+        if propagation.learned_range is not None:
+            cache[schedule_key] = (proposer, schedule)
     record = {"n_fixed": len(fixed), "n_learned": len(schedule), "accepted": True, "max_dS": 0.0, "judged": False}
     if len(schedule) == len(fixed):
         return fixed, record
     key = ("learned_judge", propagation.precision, propagation.mode, propagation.judge_tol, tuple((s.radial_start, s.radial_end) for s in schedule))
-    cache = getattr(hamiltonian, "_runner_cache", {})
     verdict = cache.get(key)
     if verdict is None:
-        probe = np.unique([energies.min(), energies.max()])
+        probe = np.unique(np.asarray(span))
         plain = replace(propagation, steps="fixed", audit=False)
         a = solve(problem, probe, potential_grid, plain, sectors=fixed)
         b = solve(problem, probe, potential_grid, plain, sectors=schedule)

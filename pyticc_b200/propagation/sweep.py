@@ -226,6 +226,7 @@ class PartialWaveSweep:
         nat.Workspace.get(self.device, max(l.workspace_bytes for l in self.launches), slot=SWEEP_WORKSPACE_SLOT)
         self.use_graph = graph
         self.graph = None
+        self.graph_launches = 0  # library kernels recorded in the graph (each replay launches them)
         logger.info(f"Partial-wave sweep: {len(self.states)} blocks in {len(self.launches)} launches, classes merged: {sorted(k for k, v in merges.items() if v)}, graph={graph}")
 
     # ---- autotuning --------------------------------------------------------------------------
@@ -319,8 +320,11 @@ class PartialWaveSweep:
                 # library sets kernel attributes and queries the device while enqueueing, which
                 # the relaxed capture mode allows.
                 self.graph = torch.cuda.CUDAGraph()
+                lib = nat.load_library()
+                before = lib.ticc_kernel_launches()
                 with torch.cuda.graph(self.graph, capture_error_mode="relaxed"):
                     self._enqueue_all()
+                self.graph_launches = int(lib.ticc_kernel_launches() - before)
         return out
     def run(self, Etot) -> list:
         """ScatteringResult per system (None for a system without channels)."""

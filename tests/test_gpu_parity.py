@@ -325,6 +325,15 @@ def test_learned_schedule_is_judged_inside_solve():
     again: dict = {}
     tb.solve(wl.system, energies, wl.grid, tb.Propagation(mode="capture", steps="learned", proposer=proposer), stats=again)
     assert not again["learned"]["judged"]  # the cached verdict
+    span = (float(wl.energies.min()), float(wl.energies.max()))
+    ranged: list = []
+    for batch in (wl.energies[[1, 2]], wl.energies[[3, 4]]):  # one schedule for the whole range
+        st: dict = {}
+        tb.solve(wl.system, batch, wl.grid, tb.Propagation(mode="capture", steps="learned", proposer=proposer, learned_range=span), stats=st)
+        ranged.append(st["learned"])
+    assert ranged[0]["n_learned"] == ranged[1]["n_learned"] and not ranged[1]["judged"]
+    with pytest.raises(ValueError, match="learned_range"):
+        tb.solve(wl.system, wl.energies[[0, 5]] * 2.0, wl.grid, tb.Propagation(mode="capture", steps="learned", proposer=proposer, learned_range=span))
     strict: dict = {}
     refused = tb.solve(wl.system, energies, wl.grid, tb.Propagation(mode="capture", steps="learned", proposer=proposer, judge_tol=1e-300), stats=strict)
     assert not strict["learned"]["accepted"] and strict["sectors"] == record["n_fixed"]
