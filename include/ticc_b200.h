@@ -92,8 +92,8 @@ int ticc_debug_set_step_poll_limit(long long polls);
  * column tile tb, device ints) it computes, in the 128 x 128 block (ta, tb) of matrix b of
  * M (batch x np x np FP64, np a multiple of 128),
  *     M_tile <- M_tile - cold[b][:, ta block]^T U[b][:, tb block]
- * with cold and U given as batch x 128 x np FP64 panels (device), split into TF32 hi/lo
- * words, the three products hi*hi + hi*lo + lo*hi accumulated in FP32 in tensor memory.  A
+ * with cold and U given as batch x 128 x np FP64 panels (device), rounded to FP32 and split
+ * into TF32 hi/lo words in shared memory, the three products hi*hi + hi*lo + lo*hi accumulated in FP32 in tensor memory.  A
  * diagonal tile (ta == tb) keeps its lower half and mirrors it into the upper half.
  * Listed tiles must be distinct. */
 int ticc_debug_tc_update_workspace_size(int np, int batch, size_t* bytes);

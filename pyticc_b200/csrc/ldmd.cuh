@@ -45,7 +45,7 @@ struct LdmdLayout {
   double* scratch;
   size_t scratch_doubles;
   int* reduced;   // [n_sector] leading sweep blocks taken in TF32x3 (mixed mode), else null
-  float* split;   // TF32 hi/lo panels of the reduced steps' tcgen05 update (mixed mode), else null
+  float* split;   // FP32 operand panels of the reduced steps' tcgen05 update (mixed mode), else null
 };
 
 // Mixed precision: a channel whose local wavenumber at the sector midpoint exceeds this

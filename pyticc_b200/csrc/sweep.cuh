@@ -685,7 +685,7 @@ __device__ inline bool step_wait(const int* f0, const int* f1, int target, int* 
 // pivot block K is strongly closed (`reduced`), U takes the same FP32-accurate TF32x3
 // product as the step's trailing update.
 // With `split` (a reduced step whose trailing update runs on tcgen05), the old rows and U of
-// this column tile also go out split into TF32 hi/lo words for the update's TMA loads.
+// this column tile also go out as FP32 panels for the update's TMA loads.
 __device__ inline void rowpanel_unit(double* Mb, int ld, int kb, int jt, const double* Pt, double* Cb, double* smem, bool reduced, float* split, int b) {
   const int k0 = kb * kBlock, c0 = jt * kBlock;
   load_cold_tile(Cb, ld, Mb, kb, jt, smem);
@@ -701,8 +701,8 @@ __device__ inline void rowpanel_unit(double* Mb, int ld, int kb, int jt, const d
   __syncthreads();
   store_tile(Mb, ld, k0, c0, smem);
   if (split != nullptr) {
-    tc_write_split(split, b, 0, ld, Cb, ld, c0, jt);          // A = the old rows K
-    tc_write_split(split, b, 2, ld, smem, kStride, 0, jt);    // B = U = P^-1 (old rows K)
+    tc_write_panel(split, b, 0, ld, Cb, ld, c0, jt);          // A = the old rows K
+    tc_write_panel(split, b, 1, ld, smem, kStride, 0, jt);    // B = U = P^-1 (old rows K)
     fence_proxy_async_global();                               // read next by TMA (async proxy)
   }
 }

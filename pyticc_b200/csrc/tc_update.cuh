@@ -2,28 +2,31 @@
 //
 // One unit computes C <- C - A^T B for a 128 x 128 FP64 tile C of a work matrix, with
 // A = the old pivot rows (cold, 128 x 128 block of columns ta) and B = U = P^-1 cold
-// (columns tb), both given pre-split as x = hi + lo in TF32 (FP32 words):
+// (columns tb), both given as FP32 panels and split in shared memory as x = hi + lo in TF32:
 //   D = A_lo B_hi + A_hi B_lo + A_hi B_hi      (FP32 accumulation in TMEM, ~2^-21 relative)
-// Operands arrive by TMA (cp.async.bulk.tensor) through a ring of kTcStages shared-memory
-// stages of kTcChunk k-rows, already in the canonical K-major no-swizzle layout; one thread
-// issues tcgen05.mma.cta_group::1.kind::tf32 (M = N = 128, K = 8 per instruction) into a
-// 128-column TMEM accumulator and commits to mbarriers that free the stages.  The FP64 C
-// tile is loaded by TMA (128-byte swizzle) into shared memory while the products run, C - D
-// is formed there (D read from TMEM with tcgen05.ld, one TMEM lane = one row), and the tile
-// goes back by TMA store.  A diagonal tile is symmetrised from its lower half before the
-// store.
+// Operand chunks of kTcChunk k-rows arrive by TMA (cp.async.bulk.tensor) in the canonical
+// K-major no-swizzle layout through a ring of kTcStages raw stages.  Warps 1-7 split a landed
+// chunk: hi = rna_tf32(x) in place, lo = rna_tf32(x - hi) into one of kTcLoBufs lo buffers.
+// Thread 0 issues the loads and tcgen05.mma.cta_group::1.kind::tf32 (M = N = 128, K = 8
+// per instruction) into a 128-column TMEM accumulator, and commits to mbarriers that free
+// the stages.  So the panels cost 4 bytes per element in global memory and on the way into
+// the SM, half of what pre-split hi/lo panels cost.  The FP64 C tile is loaded by TMA
+// (128-byte swizzle) into shared memory while the products run, C - D is formed there (D
+// read from TMEM with tcgen05.ld, one TMEM lane = one row), and the tile goes back by TMA
+// store.  A diagonal tile is symmetrised from its lower half before the store.
 //
-// Split panel layout in global memory (written by the row-panel units, read by TMA), one
-// 8 KB block per (matrix b, panel which, 128-column tile ct, 16-row k chunk kc):
-//   block = ((b * 4 + which) * (np / 128) + ct) * 8 + kc,    which = 0: A_hi, 1: A_lo, 2: B_hi, 3: B_lo
+// Panel layout in global memory (written by the row-panel units, read by TMA), one 8 KB
+// block per (matrix b, panel which, 128-column tile ct, 16-row k chunk kc):
+//   block = ((b * 2 + which) * (np / 128) + ct) * 8 + kc,    which = 0: A (old rows K), 1: B (U)
 //   element (k, c), m = c % 128, kk = k % 16, at float block * 2048 + ((m / 8) * 4 + kk / 4) * 32 + (m % 8) * 4 + kk % 4
 // i.e. 8-row x 16-byte core matrices, the four along k 128 bytes apart (LBO), the sixteen
 // 8-row groups along m 512 bytes apart (SBO): the MMA's K-major operand layout, so a block
-// is copied into shared memory as it is.
+// is copied into shared memory as it is and split there element by element.
 //
-// Every mbarrier wait is bounded (kTcSpinLimit polls, about a second); on a timeout the unit
-// raises the call's abort flag, reports kDeviceStalled, waits (bounded again) for the loads
-// and products it issued, and the CTA frees its TMEM before it exits.
+// Every mbarrier wait is bounded (kTcSpinLimit polls, about a second) and also gives up once
+// another thread of the CTA has given up; the unit then raises the call's abort flag,
+// reports kDeviceStalled, waits (bounded again) for the loads and products it issued, and
+// the CTA frees its TMEM before it exits.
 #pragma once
 
 #include <cuda.h>
@@ -36,16 +39,21 @@
 namespace ticc {
 
 constexpr int kTcChunk = 16;                                       // k rows per stage
-constexpr int kTcStages = 3;
-constexpr int kTcArrayBytes = kBlock * kTcChunk * 4;               // 8 KB: one of A_hi, A_lo, B_hi, B_lo (one split block)
+constexpr int kTcStages = 4;                                       // raw stages (A, B), hi in place
+constexpr int kTcLoBufs = 2;                                       // lo buffers (A_lo, B_lo); chunk g uses g % 2
+constexpr int kTcArrayBytes = kBlock * kTcChunk * 4;               // 8 KB: one operand's chunk (one panel block)
 constexpr int kTcArrayFloats = kTcArrayBytes / 4;
-constexpr int kTcStageBytes = 4 * kTcArrayBytes;                   // 32 KB
+constexpr int kTcStageBytes = 2 * kTcArrayBytes;                   // 16 KB: A then B
 constexpr int kTcCBytes = kBlock * kBlock * 8;                     // 128 KB FP64 C tile (8 chunks of 16 columns)
 constexpr int kTcCChunkBytes = kBlock * 16 * 8;                    // 16 KB
 constexpr int kTcStageOffset = kTcCBytes;
-constexpr int kTcBarOffset = kTcStageOffset + kTcStages * kTcStageBytes;  // 229376
-constexpr int kTcFull = 0, kTcEmpty = kTcStages, kTcAcc = 2 * kTcStages, kTcCFull = 2 * kTcStages + 1, kTcDrain = 2 * kTcStages + 2;
-constexpr int kTcBarriers = 2 * kTcStages + 3;
+constexpr int kTcLoOffset = kTcStageOffset + kTcStages * kTcStageBytes;
+constexpr int kTcBarOffset = kTcLoOffset + kTcLoBufs * kTcStageBytes;  // 229376
+constexpr int kTcConvWarps = 7;                                    // warps 1-7 split the chunks
+constexpr int kTcFull = 0, kTcEmpty = kTcStages, kTcConv = 2 * kTcStages, kTcAcc = 3 * kTcStages, kTcCFull = 3 * kTcStages + 1, kTcDrain = 3 * kTcStages + 2;
+constexpr int kTcBarriers = 3 * kTcStages + 3;
+static_assert(kTcStages % kTcLoBufs == 0, "a stage must always pair with the same lo buffer");
+static_assert(kGemmThreads == 32 * (kTcConvWarps + 1), "the units run with thread 0 issuing and warps 1-7 converting");
 constexpr int kTcTmemSlotOffset = kTcBarOffset + 8 * kTcBarriers;
 constexpr int kTcRegionBytes = kTcTmemSlotOffset + 16;
 constexpr int kTcSmemBytes = kTcRegionBytes + 1024;                // + alignment slack of the dynamic base
@@ -83,6 +91,15 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
+// The same, giving up early once *abort (a CTA-wide flag in shared memory) is set.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint32_t bar, uint32_t parity, const volatile int* abort) {
+  for (long long it = 0; it < kTcSpinLimit; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (*abort) return false;
+  }
+  return false;
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) { asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory"); }
 
 __device__ __forceinline__ void fence_proxy_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
@@ -169,13 +186,14 @@ struct TcState {
   char* base;       // 1024-aligned start of the region
   uint32_t base_u;  // its shared-window address
   uint32_t tmem;    // accumulator (lane 0, first column)
-  uint32_t chunk;   // operand chunks issued so far (thread 0's count)
+  uint32_t chunk;   // operand chunks of finished tiles (every thread keeps the count)
   uint32_t tile;    // tiles finished so far
   int nt;           // 128-column tiles per matrix (np / 128)
+  volatile int* abort;  // CTA-wide give-up flag in shared memory
 };
 
-// Split block of (matrix b, panel which, column tile ct, k chunk kc) when a matrix has nt tiles.
-__device__ __forceinline__ int tc_split_block(int b, int which, int nt, int ct, int kc) { return ((b * 4 + which) * nt + ct) * (kBlock / kTcChunk) + kc; }
+// Panel block of (matrix b, panel which, column tile ct, k chunk kc) when a matrix has nt tiles.
+__device__ __forceinline__ int tc_split_block(int b, int which, int nt, int ct, int kc) { return ((b * 2 + which) * nt + ct) * (kBlock / kTcChunk) + kc; }
 
 __device__ __forceinline__ uint32_t tc_bar(const TcState& s, int i) { return s.base_u + kTcBarOffset + 8u * (uint32_t)i; }
 
@@ -190,9 +208,11 @@ __device__ inline void tc_setup(TcState& s, void* dynamic_smem, int np) {
   s.chunk = 0;
   s.tile = 0;
   s.nt = np / kBlock;
+  s.abort = reinterpret_cast<volatile int*>(s.base + kTcTmemSlotOffset + 8);
   if (threadIdx.x == 0) {
-    for (int i = 0; i < kTcBarriers; ++i) mbar_init(tc_bar(s, i), 1);
+    for (int i = 0; i < kTcBarriers; ++i) mbar_init(tc_bar(s, i), (i >= kTcConv && i < kTcConv + kTcStages) ? kTcConvWarps : 1);
     mbar_fence_init();
+    *s.abort = 0;
   }
   if (threadIdx.x < 32) {
     tmem_alloc(s.base_u + kTcTmemSlotOffset, kTcTmemColumns);
@@ -218,38 +238,73 @@ struct TcMaps {
   CUtensorMap matrix;  // 3-D {np, np, batch} over the FP64 work matrices, box {16, 128, 1}
 };
 
-// Issue the four TMA loads of operand chunk `c` (k rows c * kTcChunk ..) of tile (ta, tb) of
-// matrix b into stage `stage`; thread 0 only.
+// x = hi + lo with hi = rna_tf32(x) and lo = rna_tf32(x - hi) (x - hi is exact in FP32)
+__device__ __forceinline__ void tc_split_value(float f, float& hi, float& lo) {
+  unsigned h, l;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(f));
+  const float rest = f - __uint_as_float(h);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(rest));
+  hi = __uint_as_float(h);
+  lo = __uint_as_float(l);
+}
+
+// Issue the two TMA loads of operand chunk `c` (k rows c * kTcChunk ..) of tile (ta, tb) of
+// matrix b into raw stage `stage`; thread 0 only.
 __device__ __forceinline__ void tc_issue_chunk(const TcState& s, const CUtensorMap* split, int b, int ta, int tb, int c, int stage) {
   const uint32_t dst = s.base_u + kTcStageOffset + (uint32_t)stage * kTcStageBytes;
   const uint32_t full = tc_bar(s, kTcFull + stage);
   mbar_expect_tx(full, kTcStageBytes);
   const int nt = s.nt;
   const uint64_t keep = l2_policy_evict_last();
-  tma_load_3d(dst + 0 * kTcArrayBytes, split, 0, 0, tc_split_block(b, 0, nt, ta, c), full, keep);
-  tma_load_3d(dst + 1 * kTcArrayBytes, split, 0, 0, tc_split_block(b, 1, nt, ta, c), full, keep);
-  tma_load_3d(dst + 2 * kTcArrayBytes, split, 0, 0, tc_split_block(b, 2, nt, tb, c), full, keep);
-  tma_load_3d(dst + 3 * kTcArrayBytes, split, 0, 0, tc_split_block(b, 3, nt, tb, c), full, keep);
+  tma_load_3d(dst, split, 0, 0, tc_split_block(b, 0, nt, ta, c), full, keep);
+  tma_load_3d(dst + kTcArrayBytes, split, 0, 0, tc_split_block(b, 1, nt, tb, c), full, keep);
+}
+
+// Split the landed raw chunk of `stage` (A then B, 1024 float4) into hi (in place) and lo
+// (lo buffer `lo`); the threads of warps 1-7, each warp arriving once on the stage's
+// conversion barrier after its writes are made visible to the tensor core's proxy.
+__device__ __forceinline__ void tc_convert_chunk(const TcState& s, int stage, int lo) {
+  float4* raw = reinterpret_cast<float4*>(s.base + kTcStageOffset + stage * kTcStageBytes);
+  float4* low = reinterpret_cast<float4*>(s.base + kTcLoOffset + lo * kTcStageBytes);
+  constexpr int kVec = kTcStageBytes / 16;  // 1024
+  for (int i = (int)threadIdx.x - 32; i < kVec; i += 32 * kTcConvWarps) {
+    const float4 x = raw[i];
+    float4 h, l;
+    tc_split_value(x.x, h.x, l.x);
+    tc_split_value(x.y, h.y, l.y);
+    tc_split_value(x.z, h.z, l.z);
+    tc_split_value(x.w, h.w, l.w);
+    raw[i] = h;
+    low[i] = l;
+  }
+  fence_proxy_async_shared();
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) mbar_arrive(tc_bar(s, kTcConv + stage));
 }
 
 // One update tile.  Returns false (on every thread) if a wait gave up; the abort flag and
 // status are then set and the unit's issued work has been drained (bounded waits).
+//
+// Chunk g (counted over the CTA's tiles, g = s.chunk + c) lives in raw stage g % kTcStages
+// and lo buffer g % kTcLoBufs.  Phases: full[stage] completes when its loads land, conv[stage]
+// when warps 1-7 have split it, empty[stage] when its MMAs have read it.  Thread 0 refills a
+// stage after its empty phase; a converter writes lo buffer g % 2 after chunk g - 2's empty
+// phase.  Every wait is for the phase right after one this thread has already waited for
+// (or the first), so the parity of a wait always names the phase it means.
 __device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int ta, int tb, int* abort_flag, int* status) {
   constexpr int nchunks = kBlock / kTcChunk;  // 8
-  __shared__ int tc_ok;
   const int tid = threadIdx.x;
   const int r0 = ta * kBlock, c0 = tb * kBlock;
+  const uint32_t g0 = s.chunk;
   if (tid == 0) {
     int ok = 1;
-    unsigned loads_pending = 0;  // stages whose TMA load was issued and not yet waited
+    unsigned loads_pending = 0;  // stages whose TMA load was issued and not yet seen complete
     uint32_t pending_parity[kTcStages] = {};
     bool c_pending = false, mma_issued = false;
     // split panels written by other CTAs of this launch were released to this thread by the
     // flag it acquired; the stages were last read by the previous unit's MMAs (waited for)
     fence_proxy_async_shared();
     fence_proxy_async_global();
-    // operand ring first: chunk g = s.chunk + c uses stage g % kTcStages in its (g / kTcStages)-th use
-    const uint32_t g0 = s.chunk;
     auto issue = [&](int c, uint32_t g) {
       const int stage = g % kTcStages;
       tc_issue_chunk(s, &maps.split, b, ta, tb, c, stage);
@@ -259,7 +314,7 @@ __device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int
     for (int c = 0; c < kTcStages && c < nchunks && ok; ++c) {
       const uint32_t g = g0 + c;
       // the MMAs that last read this stage (chunk g - kTcStages) have completed
-      if (g >= (uint32_t)kTcStages && !mbar_wait(tc_bar(s, kTcEmpty + g % kTcStages), ((g - kTcStages) / kTcStages) & 1u)) ok = 0;
+      if (g >= (uint32_t)kTcStages && !mbar_wait_or_abort(tc_bar(s, kTcEmpty + g % kTcStages), ((g - kTcStages) / kTcStages) & 1u, s.abort)) ok = 0;
       if (ok) issue(c, g);
     }
     // then the C tile, once the previous unit's TMA store has read the buffer out (its
@@ -273,21 +328,21 @@ __device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int
       for (int q = 0; q < 8; ++q) tma_load_3d(s.base_u + (uint32_t)q * kTcCChunkBytes, &maps.matrix, c0 + 16 * q, r0, b, cbar, once);
       c_pending = true;
     }
-    tc_fence_after();
     for (int c = 0; c < nchunks && ok; ++c) {
       const uint32_t g = g0 + c;
       const int stage = g % kTcStages;
-      if (!mbar_wait(tc_bar(s, kTcFull + stage), (g / kTcStages) & 1u)) {
+      if (!mbar_wait_or_abort(tc_bar(s, kTcConv + stage), (g / kTcStages) & 1u, s.abort)) {
         ok = 0;
         break;
       }
-      loads_pending &= ~(1u << stage);
+      loads_pending &= ~(1u << stage);  // split, so landed
       tc_fence_after();
       const uint32_t st = s.base_u + kTcStageOffset + (uint32_t)stage * kTcStageBytes;
+      const uint32_t lo = s.base_u + kTcLoOffset + (uint32_t)(g % kTcLoBufs) * kTcStageBytes;
 #pragma unroll
       for (int kg = 0; kg < kTcChunk / 8; ++kg) {
-        const uint64_t a_hi = tc_desc(st + 0 * kTcArrayBytes, kg), a_lo = tc_desc(st + 1 * kTcArrayBytes, kg);
-        const uint64_t b_hi = tc_desc(st + 2 * kTcArrayBytes, kg), b_lo = tc_desc(st + 3 * kTcArrayBytes, kg);
+        const uint64_t a_hi = tc_desc(st, kg), a_lo = tc_desc(lo, kg);
+        const uint64_t b_hi = tc_desc(st + kTcArrayBytes, kg), b_lo = tc_desc(lo + kTcArrayBytes, kg);
         tc_mma_tf32(s.tmem, a_lo, b_hi, (c > 0 || kg > 0) ? 1u : 0u);
         tc_mma_tf32(s.tmem, a_hi, b_lo, 1u);
         tc_mma_tf32(s.tmem, a_hi, b_hi, 1u);
@@ -297,7 +352,7 @@ __device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int
       // refill the stage of the previous chunk (its MMAs precede this chunk's in the pipe)
       if (c >= 1 && c - 1 + kTcStages < nchunks) {
         const uint32_t gp = g - 1;
-        if (!mbar_wait(tc_bar(s, kTcEmpty + gp % kTcStages), (gp / kTcStages) & 1u)) {
+        if (!mbar_wait_or_abort(tc_bar(s, kTcEmpty + gp % kTcStages), (gp / kTcStages) & 1u, s.abort)) {
           ok = 0;
           break;
         }
@@ -306,13 +361,13 @@ __device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int
     }
     if (ok) {
       tc_commit(tc_bar(s, kTcAcc));
-      s.chunk = g0 + nchunks;
       mma_issued = false;
-      if (!mbar_wait(tc_bar(s, kTcAcc), s.tile & 1u)) ok = 0;
-      if (ok && mbar_wait(cbar, s.tile & 1u)) c_pending = false;
+      if (!mbar_wait_or_abort(tc_bar(s, kTcAcc), s.tile & 1u, s.abort)) ok = 0;
+      if (ok && mbar_wait_or_abort(cbar, s.tile & 1u, s.abort)) c_pending = false;
       else ok = 0;
     }
     if (!ok) {
+      *s.abort = 1;  // the converters stop waiting
       if (atomicExch(abort_flag, 1) == 0) report_status(status, kDeviceStalled, b, -1);
       // drain: the issued loads and products land before the CTA moves on or frees TMEM
       for (int st = 0; st < kTcStages; ++st)
@@ -323,10 +378,27 @@ __device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int
         mbar_wait(tc_bar(s, kTcDrain), 0u);
       }
     }
-    tc_ok = ok;
+  } else if (tid >= 32) {
+    for (int c = 0; c < nchunks; ++c) {
+      const uint32_t g = g0 + c;
+      const int stage = g % kTcStages;
+      // the raw chunk has landed, and the MMAs of chunk g - kTcLoBufs (the lo buffer's last
+      // reader) have completed
+      bool ok = mbar_wait_or_abort(tc_bar(s, kTcFull + stage), (g / kTcStages) & 1u, s.abort);
+      if (ok && g >= (uint32_t)kTcLoBufs) {
+        const uint32_t gp = g - kTcLoBufs;
+        ok = mbar_wait_or_abort(tc_bar(s, kTcEmpty + gp % kTcStages), (gp / kTcStages) & 1u, s.abort);
+      }
+      if (!ok) {
+        *s.abort = 1;  // thread 0 stops waiting for this warp's conversion
+        break;
+      }
+      tc_convert_chunk(s, stage, g % kTcLoBufs);
+    }
   }
   __syncthreads();
-  if (!tc_ok) return false;
+  if (*s.abort) return false;
+  s.chunk = g0 + nchunks;
   // every thread observes the completed C load itself (acquire of the async-proxy writes)
   mbar_wait(tc_bar(s, kTcCFull), s.tile & 1u);
   tc_fence_after();
@@ -370,38 +442,27 @@ __device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int
   return true;
 }
 
-__device__ __forceinline__ void tc_split_value(double x, float& hi, float& lo) {
-  unsigned h, l;
-  const float f = static_cast<float>(x);
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(f));
-  const float rest = f - __uint_as_float(h);
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(rest));
-  hi = __uint_as_float(h);
-  lo = __uint_as_float(l);
-}
 
-// Write the split of one 128 x 128 block of a panel (k rows 0..127 of src at row stride ld,
-// columns src_c0 .. src_c0 + 127) into panels which_hi / which_hi + 1, column tile ct.  All
-// threads of the CTA; a thread takes 4 consecutive k of one column (coalesced loads across
-// the warp's consecutive columns) and stores them as one 16-byte row of a core matrix.
-__device__ inline void tc_write_split(float* split, int b, int which_hi, int np, const double* src, long long ld, int src_c0, int ct) {
+// Write one 128 x 128 block of a panel (k rows 0..127 of src at row stride ld, columns
+// src_c0 .. src_c0 + 127), rounded to FP32, into panel `which`, column tile ct.  All threads of
+// the CTA; a thread takes 4 consecutive k of one column (coalesced loads across the warp's
+// consecutive columns) and stores them as one 16-byte row of a core matrix.
+__device__ inline void tc_write_panel(float* split, int b, int which, int np, const double* src, long long ld, int src_c0, int ct) {
   const int nt = np / kBlock;
   for (int e = threadIdx.x; e < kBlock * (kBlock / 4); e += blockDim.x) {
     const int k4 = e / kBlock, m = e % kBlock;
     const int k = 4 * k4;
-    float hi[4], lo[4];
+    float v[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) tc_split_value(src[(long long)(k + j) * ld + src_c0 + m], hi[j], lo[j]);
+    for (int j = 0; j < 4; ++j) v[j] = static_cast<float>(src[(long long)(k + j) * ld + src_c0 + m]);
     const int kk = k % kTcChunk;
     const long long inner = ((m >> 3) * 4 + (kk >> 2)) * 32 + (m & 7) * 4;
-    const long long bh = (long long)tc_split_block(b, which_hi, nt, ct, k / kTcChunk) * kTcArrayFloats;
-    const long long bl = (long long)tc_split_block(b, which_hi + 1, nt, ct, k / kTcChunk) * kTcArrayFloats;
-    *reinterpret_cast<float4*>(split + bh + inner) = make_float4(hi[0], hi[1], hi[2], hi[3]);
-    *reinterpret_cast<float4*>(split + bl + inner) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+    const long long blk = (long long)tc_split_block(b, which, nt, ct, k / kTcChunk) * kTcArrayFloats;
+    *reinterpret_cast<float4*>(split + blk + inner) = make_float4(v[0], v[1], v[2], v[3]);
   }
 }
 
-inline size_t tc_split_floats(int np, int batch) { return size_t(4) * kBlock * (size_t)np * (size_t)batch; }
+inline size_t tc_split_floats(int np, int batch) { return size_t(2) * kBlock * (size_t)np * (size_t)batch; }
 
 // ---- host: tensor maps ----------------------------------------------------------------------------
 typedef CUresult (*TcEncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
@@ -423,7 +484,7 @@ inline cudaError_t tc_make_maps(TcMaps& maps, const float* split, const double* 
   TcEncodeTiled encode = tc_encoder();
   if (encode == nullptr) return cudaErrorNotSupported;
   if (np % kBlock != 0 || (reinterpret_cast<uintptr_t>(split) & 15) || (reinterpret_cast<uintptr_t>(M) & 15) || (mstride * 8) % 16 != 0) return cudaErrorInvalidValue;
-  const cuuint64_t blocks = (cuuint64_t)batch * 4 * (np / kBlock) * (kBlock / kTcChunk);
+  const cuuint64_t blocks = (cuuint64_t)batch * 2 * (np / kBlock) * (kBlock / kTcChunk);
   const cuuint64_t sdim[3] = {256, (cuuint64_t)(kTcArrayFloats / 256), blocks};
   const cuuint64_t sstride[2] = {256 * 4, (cuuint64_t)kTcArrayBytes};
   const cuuint32_t sbox[3] = {256, (cuuint32_t)(kTcArrayFloats / 256), 1};
@@ -443,8 +504,8 @@ inline cudaError_t tc_make_maps(TcMaps& maps, const float* split, const double* 
 // cold and U: [batch][128][np]; one CTA per (128-column block, matrix).
 __global__ void __launch_bounds__(256) tc_split_panels_kernel(const double* cold, const double* U, int np, int batch, float* split) {
   const int jt = blockIdx.x, b = blockIdx.y;
-  tc_write_split(split, b, 0, np, cold + (long long)b * kBlock * np, np, jt * kBlock, jt);
-  tc_write_split(split, b, 2, np, U + (long long)b * kBlock * np, np, jt * kBlock, jt);
+  tc_write_panel(split, b, 0, np, cold + (long long)b * kBlock * np, np, jt * kBlock, jt);
+  tc_write_panel(split, b, 1, np, U + (long long)b * kBlock * np, np, jt * kBlock, jt);
 }
 
 // tiles[3 t .. 3 t + 2] = (matrix, row tile, column tile); every CTA takes tiles t = blockIdx.x,

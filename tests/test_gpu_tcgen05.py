@@ -1,7 +1,7 @@
 """The tcgen05 TF32x3 trailing-update tile (TMA-fed, TMEM-accumulated) against FP64.
 
-C <- C - A^T B on 128 x 128 tiles with A, B split as hi + lo TF32 words and the three
-products hi*hi + hi*lo + lo*hi accumulated in FP32: the error must stay at the FP32 level
+C <- C - A^T B on 128 x 128 tiles with A, B given as FP32 panels, split in shared memory
+as hi + lo TF32 words, and the three products hi*hi + hi*lo + lo*hi accumulated in FP32: the error must stay at the FP32 level
 (bound: 1e-5 of sum |a||b| per element, mean relative error below 2e-6, far from the 1e-3
 of a single TF32 product), untouched tiles must not change, and a diagonal tile must come
 out exactly symmetric (lower half mirrored).
