@@ -226,8 +226,11 @@ __device__ inline void invert_pivot_block(double* P, double* aux, double* Mb, in
   }
 }
 
+// With `split` (a sweep whose first step runs on tcgen05: 0 < *reduced_blocks), P^-1 also goes
+// out as that step's pivot panel (slot 0) for the row-panel products.
 template <bool kSym>
-__global__ void __launch_bounds__(kPivotThreads) sweep_pivot_kernel(double* __restrict__ M, long long mstride, int ld, int k0, double* __restrict__ pinv, int* status) {
+__global__ void __launch_bounds__(kPivotThreads) sweep_pivot_kernel(double* __restrict__ M, long long mstride, int ld, int k0, double* __restrict__ pinv, int* status, float* split = nullptr,
+                                                                    const int* reduced_blocks = nullptr, int batch = 0) {
   extern __shared__ double smem[];
   double* P = smem;
   double* aux = smem + kBlock * kPivotLd;
@@ -252,6 +255,10 @@ __global__ void __launch_bounds__(kPivotThreads) sweep_pivot_kernel(double* __re
   }
   __syncthreads();
   invert_pivot_block<kSym>(P, aux, Mb, ld, k0, pinv, b, status);
+  if (split != nullptr && reduced_blocks != nullptr && 0 < *reduced_blocks) {
+    __syncthreads();
+    tc_write_panel_at(split + (long long)tc_pinv_block(b, 0, ld / kBlock, batch) * kTcArrayFloats, pinv + (long long)b * 2 * kBlock * kBlock, kBlock, 0);
+  }
 }
 
 // Sweep of a single-block matrix whose channels fill at most the leading 64 rows and
@@ -763,6 +770,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1) sweep_step_kernel(double* __r
     tc_live = true;
   }
   for (;;) {
+    // the previous unit's generic shared-memory writes come before any TMA load of the next
+    if (tensor_core) fence_proxy_async_shared();
     if (tid == 0) *slot = atomicAdd(queue, 1);
     __syncthreads();
     const int u = *slot;
@@ -772,7 +781,11 @@ __global__ void __launch_bounds__(kGemmThreads, 1) sweep_step_kernel(double* __r
       const int b = u / t, j = u % t;
       const int jt = j + (j >= kb ? 1 : 0);
       double* Mb = M + (long long)b * mstride;
-      rowpanel_unit(Mb, ld, kb, jt, pinv + (long long)b * 2 * kBlock * kBlock + pslot * kBlock * kBlock, cold + (long long)b * cstride, smem, reduced, tensor_core ? split : nullptr, b);
+      if (tc_live) {
+        if (!tc_rowpanel_unit(tcs, maps, split, tc_pinv_block(b, pslot, t + 1, batch), b, kb, jt, Mb, ld, cold + (long long)b * cstride, abort_flag, status)) tc_live = false;
+      } else {
+        rowpanel_unit(Mb, ld, kb, jt, pinv + (long long)b * 2 * kBlock * kBlock + pslot * kBlock * kBlock, cold + (long long)b * cstride, smem, reduced, tensor_core ? split : nullptr, b);
+      }
       __syncthreads();
       if (tid == 0) {
         __threadfence();
@@ -807,6 +820,11 @@ __global__ void __launch_bounds__(kGemmThreads, 1) sweep_step_kernel(double* __r
       __syncthreads();
       invert_pivot_block<true>(Cs, smem, Mb, ld, p0, pinv + nslot * kBlock * kBlock, b, status);
       __syncthreads();
+      if (split != nullptr && kb + 1 < *reduced_blocks) {  // the next step's row panels run on tcgen05
+        tc_write_panel_at(split + (long long)tc_pinv_block(b, nslot, t + 1, batch) * kTcArrayFloats, pinv + nslot * kBlock * kBlock + (long long)b * 2 * kBlock * kBlock, kBlock, 0);
+        fence_proxy_async_global();
+        __syncthreads();
+      }
       continue;
     }
     const int g = u - n_panel - n_pivot;
@@ -894,7 +912,8 @@ inline cudaError_t sweep_batched(double* M, long long mstride, int np, int batch
     e = cudaMemsetAsync(queue, 0, sizeof(int) * kStepIntsPerMatrix * (size_t)batch, stream);
     if (e != cudaSuccess) return e;
   }
-  sweep_pivot_kernel<kSym><<<batch, kPivotThreads, kPivotSmemBytes, stream>>>(M, mstride, np, 0, pinv, status);
+  const bool tc_steps = kSym && reduced_blocks != nullptr && split != nullptr && nt >= 2 && nt <= kStepIntsPerMatrix - kStepFlagOffset;
+  sweep_pivot_kernel<kSym><<<batch, kPivotThreads, kPivotSmemBytes, stream>>>(M, mstride, np, 0, pinv, status, tc_steps ? split : nullptr, reduced_blocks, batch);
   note_launch();
   if (fused) {
     TcMaps maps{};

@@ -15,13 +15,21 @@
 // read from TMEM with tcgen05.ld, one TMEM lane = one row), and the tile goes back by TMA
 // store.  A diagonal tile is symmetrised from its lower half before the store.
 //
-// Panel layout in global memory (written by the row-panel units, read by TMA), one 8 KB
-// block per (matrix b, panel which, 128-column tile ct, 16-row k chunk kc):
+// The row panels of such a step run on the same machinery (tc_rowpanel_unit): U = P^-1 cold
+// with P^-1 from a pivot panel (written by the unit that inverted the pivot) and cold, the
+// unit's FP64 tile of M loaded into the C buffer, turned into the B operand by the converter
+// warps, which write the update's A panel on the way; U leaves as FP64 (TMA store) and as the
+// update's B panel (one bulk copy).
+//
+// Panel layout in global memory (read by TMA), one 8 KB block per (matrix b, panel which,
+// 128-column tile ct, 16-row k chunk kc):
 //   block = ((b * 2 + which) * (np / 128) + ct) * 8 + kc,    which = 0: A (old rows K), 1: B (U)
 //   element (k, c), m = c % 128, kk = k % 16, at float block * 2048 + ((m / 8) * 4 + kk / 4) * 32 + (m % 8) * 4 + kk % 4
 // i.e. 8-row x 16-byte core matrices, the four along k 128 bytes apart (LBO), the sixteen
 // 8-row groups along m 512 bytes apart (SBO): the MMA's K-major operand layout, so a block
-// is copied into shared memory as it is and split there element by element.
+// is copied into shared memory as it is and split there element by element.  After the
+// panels of all matrices come two pivot panels per matrix (tc_pinv_block: P^-1[k][m] as
+// element (k, m), slot = step parity).
 //
 // Every mbarrier wait is bounded (kTcSpinLimit polls, about a second) and also gives up once
 // another thread of the CTA has given up; the unit then raises the call's abort flag,
@@ -126,6 +134,9 @@ __device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, uint32_t sr
   asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group.L2::cache_hint [%0, {%2, %3, %4}], [%1], %5;" ::"l"(reinterpret_cast<uint64_t>(map)), "r"(src),
                "r"(x), "r"(y), "r"(z), "l"(policy)
                : "memory");
+}
+__device__ __forceinline__ void bulk_copy_s2g(void* dst, uint32_t src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
@@ -248,86 +259,117 @@ __device__ __forceinline__ void tc_split_value(float f, float& hi, float& lo) {
   lo = __uint_as_float(l);
 }
 
-// Issue the two TMA loads of operand chunk `c` (k rows c * kTcChunk ..) of tile (ta, tb) of
-// matrix b into raw stage `stage`; thread 0 only.
-__device__ __forceinline__ void tc_issue_chunk(const TcState& s, const CUtensorMap* split, int b, int ta, int tb, int c, int stage) {
+// Issue the TMA loads of operand chunk `c` (k rows c * kTcChunk ..) into raw stage `stage`:
+// A from panel block a0 + c and, when b0 >= 0, B from panel block b0 + c (a row-panel unit
+// builds B itself); thread 0 only.
+__device__ __forceinline__ void tc_issue_chunk(const TcState& s, const CUtensorMap* split, int a0, int b0, int c, int stage) {
   const uint32_t dst = s.base_u + kTcStageOffset + (uint32_t)stage * kTcStageBytes;
   const uint32_t full = tc_bar(s, kTcFull + stage);
-  mbar_expect_tx(full, kTcStageBytes);
-  const int nt = s.nt;
+  mbar_expect_tx(full, b0 >= 0 ? kTcStageBytes : kTcArrayBytes);
   const uint64_t keep = l2_policy_evict_last();
-  tma_load_3d(dst, split, 0, 0, tc_split_block(b, 0, nt, ta, c), full, keep);
-  tma_load_3d(dst + kTcArrayBytes, split, 0, 0, tc_split_block(b, 1, nt, tb, c), full, keep);
+  tma_load_3d(dst, split, 0, 0, a0 + c, full, keep);
+  if (b0 >= 0) tma_load_3d(dst + kTcArrayBytes, split, 0, 0, b0 + c, full, keep);
 }
 
-// Split the landed raw chunk of `stage` (A then B, 1024 float4) into hi (in place) and lo
-// (lo buffer `lo`); the threads of warps 1-7, each warp arriving once on the stage's
-// conversion barrier after its writes are made visible to the tensor core's proxy.
-__device__ __forceinline__ void tc_convert_chunk(const TcState& s, int stage, int lo) {
+// x <- hi, returns lo, component by component.
+__device__ __forceinline__ float4 tc_split4(float4& x) {
+  float4 l;
+  tc_split_value(x.x, x.x, l.x);
+  tc_split_value(x.y, x.y, l.y);
+  tc_split_value(x.z, x.z, l.z);
+  tc_split_value(x.w, x.w, l.w);
+  return l;
+}
+
+// Split the first `vecs` float4 of the landed raw chunk of `stage` into hi (in place) and lo
+// (lo buffer `lo`); the threads of warps 1-7.
+__device__ __forceinline__ void tc_split_stage(const TcState& s, int stage, int lo, int vecs) {
   float4* raw = reinterpret_cast<float4*>(s.base + kTcStageOffset + stage * kTcStageBytes);
   float4* low = reinterpret_cast<float4*>(s.base + kTcLoOffset + lo * kTcStageBytes);
-  constexpr int kVec = kTcStageBytes / 16;  // 1024
-  for (int i = (int)threadIdx.x - 32; i < kVec; i += 32 * kTcConvWarps) {
-    const float4 x = raw[i];
-    float4 h, l;
-    tc_split_value(x.x, h.x, l.x);
-    tc_split_value(x.y, h.y, l.y);
-    tc_split_value(x.z, h.z, l.z);
-    tc_split_value(x.w, h.w, l.w);
-    raw[i] = h;
+  for (int i = (int)threadIdx.x - 32; i < vecs; i += 32 * kTcConvWarps) {
+    float4 x = raw[i];
+    const float4 l = tc_split4(x);
+    raw[i] = x;
     low[i] = l;
   }
-  fence_proxy_async_shared();
-  __syncwarp();
-  if ((threadIdx.x & 31) == 0) mbar_arrive(tc_bar(s, kTcConv + stage));
 }
 
-// One update tile.  Returns false (on every thread) if a wait gave up; the abort flag and
-// status are then set and the unit's issued work has been drained (bounded waits).
+// Element (k, n) of the FP64 tile in the C buffer, stored with rows k (`rows_k`) or rows n.
+__device__ __forceinline__ double tc_c_at(const TcState& s, bool rows_k, int k, int n) {
+  return *reinterpret_cast<const double*>(s.base + (rows_k ? tc_c_offset(k, n) : tc_c_offset(n, k)));
+}
+
+// Row-panel chunk c: B_kmajor[n][k] = cold(k, n) for the 16 k rows of the chunk, from the FP64
+// cold tile in the C buffer, split into the stage's B array (hi) and the lo buffer; the FP32
+// values also go to `out` (the update's A panel block of this chunk).  Threads of warps 1-7.
+__device__ __forceinline__ void tc_build_cold_chunk(const TcState& s, int stage, int lo, int c, bool rows_k, float* out) {
+  float* hi_b = reinterpret_cast<float*>(s.base + kTcStageOffset + stage * kTcStageBytes + kTcArrayBytes);
+  float* lo_b = reinterpret_cast<float*>(s.base + kTcLoOffset + lo * kTcStageBytes + kTcArrayBytes);
+  for (int i = (int)threadIdx.x - 32; i < kBlock * (kTcChunk / 4); i += 32 * kTcConvWarps) {
+    const int n = i & (kBlock - 1), j = i >> 7;  // k = c * 16 + 4 j .. + 3
+    const int k = c * kTcChunk + 4 * j;
+    float4 x = make_float4(static_cast<float>(tc_c_at(s, rows_k, k, n)), static_cast<float>(tc_c_at(s, rows_k, k + 1, n)), static_cast<float>(tc_c_at(s, rows_k, k + 2, n)),
+                           static_cast<float>(tc_c_at(s, rows_k, k + 3, n)));
+    const int o = ((n >> 3) * 4 + j) * 32 + (n & 7) * 4;
+    *reinterpret_cast<float4*>(out + o) = x;
+    const float4 l = tc_split4(x);
+    *reinterpret_cast<float4*>(hi_b + o) = x;
+    *reinterpret_cast<float4*>(lo_b + o) = l;
+  }
+}
+
+// The product of one unit, D = A^T B over k = 0..127 into TMEM, with the unit's FP64 tile
+// loaded by TMA into the C buffer (tile coordinates (cx, cy) of matrix b): before the operand
+// ring when `c_first` (a row-panel unit turns it into its B operand), else after it.  Thread 0
+// issues the loads and the MMAs; warps 1-7 split the chunks and, for a row-panel unit
+// (b0 < 0), build B from the tile, writing the update's A panel to `a_out` on the way.
+// Returns false on every thread if a wait gave up; the abort flag and status are then set and
+// the unit's issued work has been drained (bounded waits).
 //
-// Chunk g (counted over the CTA's tiles, g = s.chunk + c) lives in raw stage g % kTcStages
+// Chunk g (counted over the CTA's units, g = s.chunk + c) lives in raw stage g % kTcStages
 // and lo buffer g % kTcLoBufs.  Phases: full[stage] completes when its loads land, conv[stage]
 // when warps 1-7 have split it, empty[stage] when its MMAs have read it.  Thread 0 refills a
 // stage after its empty phase; a converter writes lo buffer g % 2 after chunk g - 2's empty
 // phase.  Every wait is for the phase right after one this thread has already waited for
 // (or the first), so the parity of a wait always names the phase it means.
-__device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int ta, int tb, int* abort_flag, int* status) {
+__device__ inline bool tc_product(TcState& s, const TcMaps& maps, int a0, int b0, int b, int cx, int cy, bool c_first, bool rows_k, float* a_out, int* abort_flag, int* status) {
   constexpr int nchunks = kBlock / kTcChunk;  // 8
   const int tid = threadIdx.x;
-  const int r0 = ta * kBlock, c0 = tb * kBlock;
   const uint32_t g0 = s.chunk;
+  const uint32_t cbar = tc_bar(s, kTcCFull);
   if (tid == 0) {
     int ok = 1;
     unsigned loads_pending = 0;  // stages whose TMA load was issued and not yet seen complete
     uint32_t pending_parity[kTcStages] = {};
     bool c_pending = false, mma_issued = false;
-    // split panels written by other CTAs of this launch were released to this thread by the
-    // flag it acquired; the stages were last read by the previous unit's MMAs (waited for)
+    // panels written by other CTAs of this launch were released to this thread by the flag
+    // it acquired; the stages were last read by the previous unit's MMAs (waited for)
     fence_proxy_async_shared();
     fence_proxy_async_global();
     auto issue = [&](int c, uint32_t g) {
       const int stage = g % kTcStages;
-      tc_issue_chunk(s, &maps.split, b, ta, tb, c, stage);
+      tc_issue_chunk(s, &maps.split, a0, b0, c, stage);
       loads_pending |= 1u << stage;
       pending_parity[stage] = (g / kTcStages) & 1u;
     };
+    // the tile, once the previous unit's TMA store has read the C buffer out (its generic
+    // writes were ordered before that store by a proxy fence and a barrier)
+    auto load_tile = [&]() {
+      bulk_wait_read_all();
+      fence_proxy_async_shared();
+      mbar_expect_tx(cbar, kTcCBytes);
+      const uint64_t once = l2_policy_evict_first();
+      for (int q = 0; q < 8; ++q) tma_load_3d(s.base_u + (uint32_t)q * kTcCChunkBytes, &maps.matrix, cx + 16 * q, cy, b, cbar, once);
+      c_pending = true;
+    };
+    if (c_first) load_tile();
     for (int c = 0; c < kTcStages && c < nchunks && ok; ++c) {
       const uint32_t g = g0 + c;
       // the MMAs that last read this stage (chunk g - kTcStages) have completed
       if (g >= (uint32_t)kTcStages && !mbar_wait_or_abort(tc_bar(s, kTcEmpty + g % kTcStages), ((g - kTcStages) / kTcStages) & 1u, s.abort)) ok = 0;
       if (ok) issue(c, g);
     }
-    // then the C tile, once the previous unit's TMA store has read the buffer out (its
-    // generic writes were ordered before that store by a proxy fence and a barrier)
-    const uint32_t cbar = tc_bar(s, kTcCFull);
-    if (ok) {
-      bulk_wait_read_all();
-      fence_proxy_async_shared();
-      mbar_expect_tx(cbar, kTcCBytes);
-      const uint64_t once = l2_policy_evict_first();
-      for (int q = 0; q < 8; ++q) tma_load_3d(s.base_u + (uint32_t)q * kTcCChunkBytes, &maps.matrix, c0 + 16 * q, r0, b, cbar, once);
-      c_pending = true;
-    }
+    if (ok && !c_first) load_tile();
     for (int c = 0; c < nchunks && ok; ++c) {
       const uint32_t g = g0 + c;
       const int stage = g % kTcStages;
@@ -379,29 +421,48 @@ __device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int
       }
     }
   } else if (tid >= 32) {
-    for (int c = 0; c < nchunks; ++c) {
+    // a row-panel unit reads its tile from the first chunk on
+    bool ok = b0 >= 0 || mbar_wait_or_abort(cbar, s.tile & 1u, s.abort);
+    for (int c = 0; c < nchunks && ok; ++c) {
       const uint32_t g = g0 + c;
       const int stage = g % kTcStages;
       // the raw chunk has landed, and the MMAs of chunk g - kTcLoBufs (the lo buffer's last
       // reader) have completed
-      bool ok = mbar_wait_or_abort(tc_bar(s, kTcFull + stage), (g / kTcStages) & 1u, s.abort);
+      ok = mbar_wait_or_abort(tc_bar(s, kTcFull + stage), (g / kTcStages) & 1u, s.abort);
       if (ok && g >= (uint32_t)kTcLoBufs) {
         const uint32_t gp = g - kTcLoBufs;
         ok = mbar_wait_or_abort(tc_bar(s, kTcEmpty + gp % kTcStages), (gp / kTcStages) & 1u, s.abort);
       }
-      if (!ok) {
-        *s.abort = 1;  // thread 0 stops waiting for this warp's conversion
-        break;
+      if (!ok) break;
+      const int lo = g % kTcLoBufs;
+      if (b0 >= 0) {
+        tc_split_stage(s, stage, lo, kTcStageBytes / 16);
+      } else {
+        tc_split_stage(s, stage, lo, kTcArrayBytes / 16);
+        tc_build_cold_chunk(s, stage, lo, c, rows_k, a_out + c * kTcArrayFloats);
+        fence_proxy_async_global();  // the A panel is read next by other CTAs' TMA loads
       }
-      tc_convert_chunk(s, stage, g % kTcLoBufs);
+      fence_proxy_async_shared();  // the split chunk is read next by the tensor core
+      __syncwarp();
+      if ((tid & 31) == 0) mbar_arrive(tc_bar(s, kTcConv + stage));
     }
+    if (!ok) *s.abort = 1;  // thread 0 stops waiting for this warp's conversion
   }
   __syncthreads();
   if (*s.abort) return false;
   s.chunk = g0 + nchunks;
-  // every thread observes the completed C load itself (acquire of the async-proxy writes)
-  mbar_wait(tc_bar(s, kTcCFull), s.tile & 1u);
+  // every thread observes the completed tile load itself (acquire of the async-proxy writes)
+  mbar_wait(cbar, s.tile & 1u);
   tc_fence_after();
+  return true;
+}
+
+// One update tile C <- C - A^T B: C = tile (ta, tb) of matrix b, A = the A panel of column tile
+// ta, B = the B panel of column tile tb.  Returns false (on every thread) if a wait gave up.
+__device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int ta, int tb, int* abort_flag, int* status) {
+  const int tid = threadIdx.x;
+  const int r0 = ta * kBlock, c0 = tb * kBlock;
+  if (!tc_product(s, maps, tc_split_block(b, 0, s.nt, ta, 0), tc_split_block(b, 1, s.nt, tb, 0), b, c0, r0, false, true, nullptr, abort_flag, status)) return false;
   // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (one row each), columns of half w / 4
   const int warp = tid >> 5, lane = tid & 31;
   const int r = 32 * (warp & 3) + lane;
@@ -442,13 +503,82 @@ __device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int
   return true;
 }
 
+// Row panel of a tensor-core step for column tile jt of matrix b: U = P^-1 cold on tcgen05,
+// with cold = the old rows K over the tile (tile (kb, jt) of M for jt < kb, the transpose of
+// the lower tile (jt, kb) for jt > kb) and P^-1 from the pivot panel at pinv_block0.  Writes
+// the update's A panel (cold) and B panel (U) of column tile jt, U into that lower tile and,
+// for jt = kb + 1, the old rows into `Cb` and U into the rows K (both read by the next
+// pivot's update later in this launch).  Ends with every store complete.
+__device__ inline bool tc_rowpanel_unit(TcState& s, const TcMaps& maps, float* split, int pinv_block0, int b, int kb, int jt, double* Mb, long long ld, double* Cb, int* abort_flag,
+                                        int* status) {
+  const int tid = threadIdx.x;
+  const int k0 = kb * kBlock, c0 = jt * kBlock;
+  const bool rows_k = jt < kb;  // the tile in the C buffer: (kb, jt) (rows k) or (jt, kb) (rows n)
+  const int cx = rows_k ? c0 : k0, cy = rows_k ? k0 : c0;
+  float* a_panel = split + (long long)tc_split_block(b, 0, s.nt, jt, 0) * kTcArrayFloats;
+  if (!tc_product(s, maps, pinv_block0, -1, b, cx, cy, true, rows_k, a_panel, abort_flag, status)) return false;
+  const bool pivot_next = jt == kb + 1;
+  if (pivot_next) {  // the old rows over tile kb + 1: cold[k][c0 + n]
+    for (int e = tid; e < kBlock * kBlock; e += blockDim.x) {
+      const int k = e >> 7, n = e & (kBlock - 1);
+      Cb[(long long)k * ld + c0 + n] = tc_c_at(s, rows_k, k, n);
+    }
+  }
+  __syncthreads();
+  // U = D from TMEM into the C buffer as FP64, oriented like the tile it replaces
+  const int warp = tid >> 5, lane = tid & 31;
+  const int m = 32 * (warp & 3) + lane;  // row of U (k within the pivot block)
+  const int half = warp >> 2;
+#pragma unroll 1
+  for (int q = 0; q < 4; ++q) {
+    const int col = 64 * half + 16 * q;
+    float d[16];
+    tc_ld_16(s.tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)col, d);
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const int n = col + u;
+      *reinterpret_cast<double*>(s.base + (rows_k ? tc_c_offset(m, n) : tc_c_offset(n, m))) = (double)d[u];
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  // the B panel (U rounded to FP32) into the free stage area for one bulk copy, and U into the
+  // rows K for the pivot unit
+  float* b_stage = reinterpret_cast<float*>(s.base + kTcStageOffset);
+  for (int e = tid; e < kBlock * (kBlock / 4); e += blockDim.x) {
+    const int n = e & (kBlock - 1), k = 4 * (e >> 7);
+    const int kk = k % kTcChunk;
+    const float4 v = make_float4(static_cast<float>(tc_c_at(s, rows_k, k, n)), static_cast<float>(tc_c_at(s, rows_k, k + 1, n)), static_cast<float>(tc_c_at(s, rows_k, k + 2, n)),
+                                 static_cast<float>(tc_c_at(s, rows_k, k + 3, n)));
+    *reinterpret_cast<float4*>(b_stage + (k / kTcChunk) * kTcArrayFloats + ((n >> 3) * 4 + (kk >> 2)) * 32 + (n & 7) * 4) = v;
+  }
+  if (pivot_next) {
+    for (int e = tid; e < kBlock * kBlock; e += blockDim.x) {
+      const int k = e >> 7, n = e & (kBlock - 1);
+      Mb[(long long)(k0 + k) * ld + c0 + n] = tc_c_at(s, rows_k, k, n);
+    }
+  }
+  fence_proxy_async_shared();
+  __syncthreads();
+  if (tid == 0) {
+    const uint64_t once = l2_policy_evict_first();
+    for (int q = 0; q < 8; ++q) tma_store_3d(&maps.matrix, s.base_u + (uint32_t)q * kTcCChunkBytes, cx + 16 * q, cy, b, once);
+    bulk_copy_s2g(split + (long long)tc_split_block(b, 1, s.nt, jt, 0) * kTcArrayFloats, s.base_u + kTcStageOffset, kTcStages * kTcStageBytes);
+    bulk_commit();
+    bulk_wait_all();  // written before the unit's flag is released, and the buffers free
+    fence_proxy_async_global();
+  }
+  ++s.tile;
+  __syncthreads();
+  return true;
+}
 
 // Write one 128 x 128 block of a panel (k rows 0..127 of src at row stride ld, columns
-// src_c0 .. src_c0 + 127), rounded to FP32, into panel `which`, column tile ct.  All threads of
-// the CTA; a thread takes 4 consecutive k of one column (coalesced loads across the warp's
-// consecutive columns) and stores them as one 16-byte row of a core matrix.
-__device__ inline void tc_write_panel(float* split, int b, int which, int np, const double* src, long long ld, int src_c0, int ct) {
-  const int nt = np / kBlock;
+// src_c0 .. src_c0 + 127), rounded to FP32, into the 8 panel blocks from blk0 on (k chunk kc
+// in block kc).  All threads of the CTA; a thread takes 4 consecutive k of one column
+// (coalesced loads across the warp's consecutive columns) and stores them as one 16-byte row
+// of a core matrix.
+__device__ inline void tc_write_panel_at(float* blk0, const double* src, long long ld, int src_c0) {
   for (int e = threadIdx.x; e < kBlock * (kBlock / 4); e += blockDim.x) {
     const int k4 = e / kBlock, m = e % kBlock;
     const int k = 4 * k4;
@@ -457,12 +587,20 @@ __device__ inline void tc_write_panel(float* split, int b, int which, int np, co
     for (int j = 0; j < 4; ++j) v[j] = static_cast<float>(src[(long long)(k + j) * ld + src_c0 + m]);
     const int kk = k % kTcChunk;
     const long long inner = ((m >> 3) * 4 + (kk >> 2)) * 32 + (m & 7) * 4;
-    const long long blk = (long long)tc_split_block(b, which, nt, ct, k / kTcChunk) * kTcArrayFloats;
-    *reinterpret_cast<float4*>(split + blk + inner) = make_float4(v[0], v[1], v[2], v[3]);
+    *reinterpret_cast<float4*>(blk0 + (long long)(k / kTcChunk) * kTcArrayFloats + inner) = make_float4(v[0], v[1], v[2], v[3]);
   }
 }
+// The same into panel `which` of column tile ct of matrix b.
+__device__ inline void tc_write_panel(float* split, int b, int which, int np, const double* src, long long ld, int src_c0, int ct) {
+  tc_write_panel_at(split + (long long)tc_split_block(b, which, np / kBlock, ct, 0) * kTcArrayFloats, src, ld, src_c0);
+}
 
-inline size_t tc_split_floats(int np, int batch) { return size_t(2) * kBlock * (size_t)np * (size_t)batch; }
+// After the A and B panels of all `batch` matrices come two pivot panels per matrix (P^-1 as
+// the row-panel product's A operand; slot = step parity): the first of their 8 blocks.
+__host__ __device__ inline int tc_pinv_block(int b, int slot, int nt, int batch) { return batch * 2 * nt * (kBlock / kTcChunk) + (b * 2 + slot) * (kBlock / kTcChunk); }
+inline size_t tc_split_blocks(int np, int batch) { return (size_t)tc_pinv_block(batch, 0, np / kBlock, batch); }
+
+inline size_t tc_split_floats(int np, int batch) { return tc_split_blocks(np, batch) * kTcArrayFloats; }
 
 // ---- host: tensor maps ----------------------------------------------------------------------------
 typedef CUresult (*TcEncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
@@ -484,7 +622,7 @@ inline cudaError_t tc_make_maps(TcMaps& maps, const float* split, const double* 
   TcEncodeTiled encode = tc_encoder();
   if (encode == nullptr) return cudaErrorNotSupported;
   if (np % kBlock != 0 || (reinterpret_cast<uintptr_t>(split) & 15) || (reinterpret_cast<uintptr_t>(M) & 15) || (mstride * 8) % 16 != 0) return cudaErrorInvalidValue;
-  const cuuint64_t blocks = (cuuint64_t)batch * 2 * (np / kBlock) * (kBlock / kTcChunk);
+  const cuuint64_t blocks = (cuuint64_t)tc_split_blocks(np, batch);
   const cuuint64_t sdim[3] = {256, (cuuint64_t)(kTcArrayFloats / 256), blocks};
   const cuuint64_t sstride[2] = {256 * 4, (cuuint64_t)kTcArrayBytes};
   const cuuint32_t sbox[3] = {256, (cuuint32_t)(kTcArrayFloats / 256), 1};
