@@ -686,6 +686,298 @@ __device__ inline bool step_wait(const int* f0, const int* f1, int target, int* 
   return ok;
 }
 
+// ---- streamed update phase of a tensor-core step ------------------------------------------------
+// Once a CTA of a reduced step has claimed its first trailing-update unit, it stops working unit
+// by unit and streams every further update unit it can claim through warp-specialised roles:
+//   thread 0   claims units, waits for their row-panel flags, keeps the operand ring full across
+//              unit boundaries (chunk g of the CTA in stage g % 4, as in tc_product) and issues
+//              the MMAs into TMEM accumulator j % 2 of unit j;
+//   warps 1-3  split the landed chunks into TF32 hi/lo;
+//   warps 4-7  run the epilogues (one TMEM lane = one row each): C <- C - D in the C buffer, then
+//              their leader (thread 128) stores the tile by TMA and, once the store has read
+//              the buffer, loads the next unit's C tile into it.
+// So unit j + 1's loads and products overlap unit j's epilogue and store.  Units reach the
+// roles through a ring of kTcDescSlots descriptors (b < 0 ends the stream).  Every wait is
+// bounded and gives up once another thread of the CTA has; decisions are warp-uniform, and
+// the roles meet only in mbarriers, so a role that gives up leaves no other waiting for ever.
+struct TcUnitDesc {
+  int b, ta, tb, pad;
+};
+
+__device__ __forceinline__ volatile TcUnitDesc* tc_desc_slot(const TcState& s, int j) { return reinterpret_cast<volatile TcUnitDesc*>(s.base + kTcDescOffset) + (j % kTcDescSlots); }
+
+// Bounded poll of two row-panel flags by one thread (thread 0 of the streaming CTA).
+__device__ inline bool tc_flags_ready(const int* fa, const int* fb, int target, int* abort_flag, int* status, int b) {
+  const long long limit = g_step_poll_limit;
+  for (long long it = 0;; ++it) {
+    if (it >= limit || load_acquire(abort_flag) != 0) {
+      if (atomicExch(abort_flag, 1) == 0) report_status(status, kDeviceStalled, b, target);
+      return false;
+    }
+    if (load_acquire(fa) >= target && load_acquire(fb) >= target) return true;
+    __nanosleep(128);
+  }
+}
+
+// Issue the TMA loads of the C tile of unit d into the C buffer (the leader of the epilogue warps).
+__device__ __forceinline__ void tc_stream_load_c(const TcState& s, const TcMaps& maps, const TcUnitDesc& d) {
+  const uint32_t cbar = tc_bar(s, kTcCFull);
+  fence_proxy_async_shared();
+  mbar_expect_tx(cbar, kTcCBytes);
+  const uint64_t once = l2_policy_evict_first();
+  for (int q = 0; q < 8; ++q) tma_load_3d(s.base_u + (uint32_t)q * kTcCChunkBytes, &maps.matrix, d.tb * kBlock + 16 * q, d.ta * kBlock, d.b, cbar, once);
+}
+
+// Unit (b0, ta0, tb0) has been claimed and its flags acquired by the whole CTA; the rest of the
+// step's queue (units first_update .. total - 1) is claimed here.  Returns false (on every
+// thread) if a wait gave up: the abort flag and status are then set and the issued work has
+// been drained.
+__device__ inline bool tc_update_stream(TcState& s, const TcMaps& maps, int b0, int ta0, int tb0, int* queue, int first_update, int total, int per, int t, int kb, bool fuse_next,
+                                        const int* ints, int* abort_flag, int* status) {
+  constexpr int nchunks = kBlock / kTcChunk;  // 8
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t g0 = s.chunk, tile0 = s.tile;
+  const uint32_t cbar = tc_bar(s, kTcCFull);
+  if (tid == 0) {
+    // ---- producer and MMA issuer
+    int ok = 1, n_units = 0;
+    bool ended = false, mma_issued = false;
+    unsigned loads_pending = 0;  // stages whose TMA load was issued and not yet seen split
+    uint32_t pending_parity[kTcStages] = {};
+    TcUnitDesc units[kTcDescSlots];
+    auto publish = [&](int j, int b, int ta, int tb) -> bool {
+      // the slot's previous descriptor (unit j - kTcDescSlots) has been read by every role
+      if (j >= kTcDescSlots && !mbar_wait_or_abort(tc_bar(s, kTcDescEmpty + j % kTcDescSlots), ((j - kTcDescSlots) / kTcDescSlots) & 1u, s.abort)) return false;
+      volatile TcUnitDesc* d = tc_desc_slot(s, j);
+      d->b = b;
+      d->ta = ta;
+      d->tb = tb;
+      mbar_arrive(tc_bar(s, kTcDescFull + j % kTcDescSlots));
+      return true;
+    };
+    // claim units until unit j exists or the queue is empty
+    auto ensure = [&](int j) -> bool {
+      while (ok && !ended && n_units <= j) {
+        const int u = atomicAdd(queue, 1);
+        if (u >= total) {
+          ended = true;
+          if (!publish(n_units, -1, 0, 0)) ok = 0;
+          break;
+        }
+        int b, ta, tb;
+        update_tile_of<true>(u - first_update, per, t, kb, b, ta, tb);
+        if (fuse_next && ta == kb + 1 && tb == kb + 1) continue;  // the pivot unit's tile
+        const int* fl = ints + b * kStepIntsPerMatrix + kStepFlagOffset;
+        if (!tc_flags_ready(fl + ta, fl + tb, kb + 1, abort_flag, status, b)) {
+          ok = 0;
+          break;
+        }
+        fence_proxy_async_global();  // the released panels are read next by TMA
+        units[n_units % kTcDescSlots] = TcUnitDesc{b, ta, tb, 0};
+        if (!publish(n_units, b, ta, tb)) {
+          ok = 0;
+          break;
+        }
+        ++n_units;
+      }
+      return ok && j < n_units;
+    };
+    // issue chunk g (unit (g - g0) / 8) if that unit exists; false if it does not or a wait gave up
+    auto issue = [&](uint32_t g) -> bool {
+      const int j = (int)((g - g0) / nchunks), c = (int)((g - g0) % nchunks);
+      if (!ensure(j)) return false;
+      const int stage = g % kTcStages;
+      if (g >= (uint32_t)kTcStages && !mbar_wait_or_abort(tc_bar(s, kTcEmpty + stage), ((g - kTcStages) / kTcStages) & 1u, s.abort)) {
+        ok = 0;
+        return false;
+      }
+      const TcUnitDesc& d = units[j % kTcDescSlots];
+      tc_issue_chunk(s, &maps.split, tc_split_block(d.b, 0, s.nt, d.ta, 0), tc_split_block(d.b, 1, s.nt, d.tb, 0), c, stage);
+      loads_pending |= 1u << stage;
+      pending_parity[stage] = (g / kTcStages) & 1u;
+      return true;
+    };
+    fence_proxy_async_shared();
+    fence_proxy_async_global();
+    units[0] = TcUnitDesc{b0, ta0, tb0, 0};
+    if (publish(0, b0, ta0, tb0)) n_units = 1;
+    else ok = 0;
+    for (int k = 0; k < kTcStages && ok; ++k)
+      if (!issue(g0 + k)) break;
+    for (uint32_t g = g0; ok; ++g) {
+      const int j = (int)((g - g0) / nchunks), c = (int)((g - g0) % nchunks);
+      if (j >= n_units) break;  // the queue is empty: every claimed unit has been multiplied
+      const int stage = g % kTcStages;
+      if (!mbar_wait_or_abort(tc_bar(s, kTcConv + stage), (g / kTcStages) & 1u, s.abort)) {
+        ok = 0;
+        break;
+      }
+      loads_pending &= ~(1u << stage);
+      // accumulator j % 2 has been read out by the epilogue of unit j - 2
+      if (c == 0 && j >= 2 && !mbar_wait_or_abort(tc_bar(s, kTcAccEmpty + (j & 1)), ((j - 2) / 2) & 1u, s.abort)) {
+        ok = 0;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t d_tmem = s.tmem + (uint32_t)((j & 1) * kBlock);
+      const uint32_t st = s.base_u + kTcStageOffset + (uint32_t)stage * kTcStageBytes;
+      const uint32_t lo = s.base_u + kTcLoOffset + (uint32_t)(g % kTcLoBufs) * kTcStageBytes;
+#pragma unroll
+      for (int kg = 0; kg < kTcChunk / 8; ++kg) {
+        const uint64_t a_hi = tc_desc(st, kg), a_lo = tc_desc(lo, kg);
+        const uint64_t b_hi = tc_desc(st + kTcArrayBytes, kg), b_lo = tc_desc(lo + kTcArrayBytes, kg);
+        tc_mma_tf32(d_tmem, a_lo, b_hi, (c > 0 || kg > 0) ? 1u : 0u);
+        tc_mma_tf32(d_tmem, a_hi, b_lo, 1u);
+        tc_mma_tf32(d_tmem, a_hi, b_hi, 1u);
+      }
+      mma_issued = true;
+      tc_commit(tc_bar(s, kTcEmpty + stage));
+      if (c == nchunks - 1) tc_commit(tc_bar(s, kTcAccFull + (j & 1)));
+      // refill: chunk g + 3 into the stage of chunk g - 1 (its MMAs precede this chunk's)
+      if (g >= g0 + 1) issue(g + kTcStages - 1);
+    }
+    if (!ok) {
+      *s.abort = 1;  // the other roles stop waiting
+      if (atomicExch(abort_flag, 1) == 0) report_status(status, kDeviceStalled, -1, -1);
+      for (int st = 0; st < kTcStages; ++st)
+        if (loads_pending & (1u << st)) mbar_wait(tc_bar(s, kTcFull + st), pending_parity[st]);
+      if (mma_issued) {
+        tc_commit(tc_bar(s, kTcDrain));
+        mbar_wait(tc_bar(s, kTcDrain), 0u);
+      }
+    }
+  } else if (warp >= 1 && warp <= kTcStreamConvWarps) {
+    // ---- warps 1-3: split the chunks of every unit (lanes 1-31 of warp 0 have no role)
+    bool ok = true;
+    for (int j = 0; ok; ++j) {
+      ok = __all_sync(0xffffffffu, mbar_wait_or_abort(tc_bar(s, kTcDescFull + j % kTcDescSlots), (j / kTcDescSlots) & 1u, s.abort));
+      if (!ok) break;
+      const int b = tc_desc_slot(s, j)->b;
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tc_bar(s, kTcDescEmpty + j % kTcDescSlots));
+      if (b < 0) break;
+      for (int c = 0; c < nchunks; ++c) {
+        const uint32_t g = g0 + (uint32_t)(j * nchunks + c);
+        const int stage = g % kTcStages;
+        bool w = mbar_wait_or_abort(tc_bar(s, kTcFull + stage), (g / kTcStages) & 1u, s.abort);
+        if (w && g >= (uint32_t)kTcLoBufs) {
+          const uint32_t gp = g - kTcLoBufs;
+          w = mbar_wait_or_abort(tc_bar(s, kTcEmpty + gp % kTcStages), (gp / kTcStages) & 1u, s.abort);
+        }
+        if (!__all_sync(0xffffffffu, w)) {
+          ok = false;
+          break;
+        }
+        tc_split_stage(s, stage, g % kTcLoBufs, kTcStageBytes / 16, 32 * kTcStreamConvWarps);
+        fence_proxy_async_shared();  // read next by the tensor core
+        __syncwarp();
+        // the conversion barrier counts kTcConvWarps warp arrivals: warp 1 stands in for the rest
+        if (lane == 0) mbar_arrive_count(tc_bar(s, kTcConv + stage), warp == 1 ? kTcConvWarps - (kTcStreamConvWarps - 1) : 1);
+      }
+    }
+    if (!ok) *s.abort = 1;
+  } else if (warp > kTcStreamConvWarps) {
+    // ---- warps 4-7: epilogues; thread 128 also moves the C tiles
+    const bool leader = tid == 32 * (kTcStreamConvWarps + 1);
+    const int r = 32 * (warp & 3) + lane;  // TMEM lane = tile row of this thread
+    bool ok = true, c_pending = false;
+    uint32_t c_phase = 0;
+    for (int j = 0; ok; ++j) {
+      ok = __all_sync(0xffffffffu, mbar_wait_or_abort(tc_bar(s, kTcDescFull + j % kTcDescSlots), (j / kTcDescSlots) & 1u, s.abort));
+      if (!ok) break;
+      TcUnitDesc d;
+      d.b = tc_desc_slot(s, j)->b;
+      d.ta = tc_desc_slot(s, j)->ta;
+      d.tb = tc_desc_slot(s, j)->tb;
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tc_bar(s, kTcDescEmpty + j % kTcDescSlots));
+      if (d.b < 0) break;
+      if (leader && j == 0) {  // the C buffer is free: earlier units of this CTA left no store pending
+        tc_stream_load_c(s, maps, d);
+        c_pending = true;
+        c_phase = tile0 & 1u;
+      }
+      bool w = mbar_wait_or_abort(tc_bar(s, kTcAccFull + (j & 1)), (j / 2) & 1u, s.abort);
+      if (w) w = mbar_wait_or_abort(cbar, (tile0 + (uint32_t)j) & 1u, s.abort);
+      if (!__all_sync(0xffffffffu, w)) {
+        ok = false;
+        break;
+      }
+      if (leader) c_pending = false;
+      tc_fence_after();
+      const uint32_t row_tmem = s.tmem + (uint32_t)((j & 1) * kBlock) + ((uint32_t)(32 * (warp & 3)) << 16);
+      const bool diagonal = d.ta == d.tb;
+#pragma unroll 1
+      for (int q = 0; q < kBlock / 16; ++q) {
+        const int col = 16 * q;
+        float dv[16];
+        tc_ld_16(row_tmem + (uint32_t)col, dv);
+        if (!diagonal) {
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            double2* p = reinterpret_cast<double2*>(s.base + tc_c_offset(r, col + 2 * u));
+            double2 v = *p;
+            v.x -= (double)dv[2 * u];
+            v.y -= (double)dv[2 * u + 1];
+            *p = v;
+          }
+        } else if (col <= r) {
+          // a diagonal tile keeps its lower half and mirrors it: row r writes (r, n) and
+          // (n, r) for n <= r; the upper elements of row r are written by the rows below
+#pragma unroll
+          for (int u = 0; u < 16; ++u) {
+            const int n = col + u;
+            if (n <= r) {
+              double* p = reinterpret_cast<double*>(s.base + tc_c_offset(r, n));
+              const double v = *p - (double)dv[u];
+              *p = v;
+              *reinterpret_cast<double*>(s.base + tc_c_offset(n, r)) = v;
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      fence_proxy_async_shared();  // the rows are read next by the TMA store
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(tc_bar(s, kTcAccEmpty + (j & 1)));
+        mbar_arrive(tc_bar(s, kTcEpiDone));
+      }
+      if (leader) {
+        // every epilogue warp has written its rows: store the tile, then load the next one
+        bool l = mbar_wait_or_abort(tc_bar(s, kTcEpiDone), (uint32_t)j & 1u, s.abort);
+        if (l) {
+          const uint64_t once = l2_policy_evict_first();
+          for (int q = 0; q < 8; ++q) tma_store_3d(&maps.matrix, s.base_u + (uint32_t)q * kTcCChunkBytes, d.tb * kBlock + 16 * q, d.ta * kBlock, d.b, once);
+          bulk_commit();
+          l = mbar_wait_or_abort(tc_bar(s, kTcDescFull + (j + 1) % kTcDescSlots), ((j + 1) / kTcDescSlots) & 1u, s.abort);
+        }
+        if (l) {
+          TcUnitDesc nd;
+          nd.b = tc_desc_slot(s, j + 1)->b;
+          nd.ta = tc_desc_slot(s, j + 1)->ta;
+          nd.tb = tc_desc_slot(s, j + 1)->tb;
+          if (nd.b >= 0) {
+            bulk_wait_read_all();  // the store has read the buffer
+            tc_stream_load_c(s, maps, nd);
+            c_pending = true;
+            c_phase = (tile0 + (uint32_t)j + 1) & 1u;
+          }
+        }
+        ok = l;
+      }
+      ok = __all_sync(0xffffffffu, ok);
+    }
+    if (leader) {
+      bulk_wait_all();  // this thread's stores are complete before the CTA moves on
+      if (c_pending) mbar_wait(cbar, c_phase);
+    }
+    if (!ok) *s.abort = 1;
+  }
+  __syncthreads();
+  return *s.abort == 0;
+}
+
 // Row-panel tile (b, jt) of step kb: keep the old rows K in `cold`, U = P^-1 M_KR, U into
 // the rows K and, where (jt, kb) is a lower tile, U^T into the columns K.  Pt is this
 // matrix's P^-1 for the step.  When the
@@ -837,10 +1129,13 @@ __global__ void __launch_bounds__(kGemmThreads, 1) sweep_step_kernel(double* __r
     double* Mb = M + (long long)b * mstride;
     const double* Cb = cold + (long long)b * cstride;
     if (tensor_core) {
-      // units come in queue order (row panels, pivots, then updates), so no unit that
-      // overwrites shared memory follows a tcgen05 unit whose C store may still be reading it;
-      // after a failed unit this CTA's tensor-core state is unknown: it only drains the queue
-      if (tc_live && !tc_update_unit(tcs, maps, b, ta, tb, abort_flag, status)) tc_live = false;
+      // units come in queue order (row panels, pivots, then updates): from its first update
+      // unit on, the CTA streams the rest of the queue's update units; after a failure this
+      // CTA's tensor-core state is unknown and it only drains the queue
+      if (tc_live) {
+        if (!tc_update_stream(tcs, maps, b, ta, tb, queue, n_panel + n_pivot, total, per, t, kb, fuse_next != 0, ints, abort_flag, status)) tc_live = false;
+        break;
+      }
     } else if (reduced) {
       update_unit_split(Mb, ld, k0, ta * kBlock, tb * kBlock, Cb, smem);
     } else {

@@ -59,13 +59,21 @@ constexpr int kTcLoOffset = kTcStageOffset + kTcStages * kTcStageBytes;
 constexpr int kTcBarOffset = kTcLoOffset + kTcLoBufs * kTcStageBytes;  // 229376
 constexpr int kTcConvWarps = 7;                                    // warps 1-7 split the chunks
 constexpr int kTcFull = 0, kTcEmpty = kTcStages, kTcConv = 2 * kTcStages, kTcAcc = 3 * kTcStages, kTcCFull = 3 * kTcStages + 1, kTcDrain = 3 * kTcStages + 2;
-constexpr int kTcBarriers = 3 * kTcStages + 3;
+// the streamed update phase (tc_update_stream): two TMEM accumulators, a ring of unit
+// descriptors, and the epilogue warps' hand-over of a finished C tile to its store
+constexpr int kTcDescSlots = 4;
+constexpr int kTcAccFull = 3 * kTcStages + 3, kTcAccEmpty = kTcAccFull + 2, kTcDescFull = kTcAccEmpty + 2, kTcDescEmpty = kTcDescFull + kTcDescSlots, kTcEpiDone = kTcDescEmpty + kTcDescSlots;
+constexpr int kTcBarriers = kTcEpiDone + 1;
+constexpr int kTcEpiWarps = 4;     // warps 4-7 (TMEM lanes 0-127) in the streamed phase
+constexpr int kTcStreamConvWarps = 3;  // warps 1-3 split the chunks there
 static_assert(kTcStages % kTcLoBufs == 0, "a stage must always pair with the same lo buffer");
 static_assert(kGemmThreads == 32 * (kTcConvWarps + 1), "the units run with thread 0 issuing and warps 1-7 converting");
-constexpr int kTcTmemSlotOffset = kTcBarOffset + 8 * kTcBarriers;
-constexpr int kTcRegionBytes = kTcTmemSlotOffset + 16;
+static_assert(kTcStreamConvWarps + kTcEpiWarps + 1 == kGemmThreads / 32 && kTcEpiWarps == 4, "the streamed phase: warp 0 issues, then converter warps, then four epilogue warps (TMEM lanes 0-127)");
+constexpr int kTcTmemSlotOffset = kTcBarOffset + 8 * kTcBarriers;   // TMEM address, then the abort flag at + 8
+constexpr int kTcDescOffset = kTcTmemSlotOffset + 16;                // kTcDescSlots x 16 bytes
+constexpr int kTcRegionBytes = kTcDescOffset + 16 * kTcDescSlots;
 constexpr int kTcSmemBytes = kTcRegionBytes + 1024;                // + alignment slack of the dynamic base
-constexpr int kTcTmemColumns = 128;
+constexpr int kTcTmemColumns = 256;  // two 128-column FP32 accumulators
 constexpr long long kTcSpinLimit = 1LL << 20;                      // try_wait polls (each may suspend briefly): about a second
 // instruction descriptor: D F32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12 = 2), A and B
 // K-major (bits 15, 16 clear), N = 128 (bits 17-22 = N >> 3), M = 128 (bits 24-28 = M >> 4)
@@ -108,6 +116,9 @@ __device__ __forceinline__ bool mbar_wait_or_abort(uint32_t bar, uint32_t parity
   return false;
 }
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) { asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory"); }
+__device__ __forceinline__ void mbar_arrive_count(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
 
 __device__ __forceinline__ void fence_proxy_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
@@ -221,7 +232,14 @@ __device__ inline void tc_setup(TcState& s, void* dynamic_smem, int np) {
   s.nt = np / kBlock;
   s.abort = reinterpret_cast<volatile int*>(s.base + kTcTmemSlotOffset + 8);
   if (threadIdx.x == 0) {
-    for (int i = 0; i < kTcBarriers; ++i) mbar_init(tc_bar(s, i), (i >= kTcConv && i < kTcConv + kTcStages) ? kTcConvWarps : 1);
+    for (int i = 0; i < kTcBarriers; ++i) {
+      uint32_t count = 1;
+      if (i >= kTcConv && i < kTcConv + kTcStages) count = kTcConvWarps;            // a warp-level arrival of every converter warp
+      if (i >= kTcAccEmpty && i < kTcAccEmpty + 2) count = kTcEpiWarps;             // every epilogue warp has read the accumulator
+      if (i >= kTcDescEmpty && i < kTcDescEmpty + kTcDescSlots) count = kTcStreamConvWarps + kTcEpiWarps;  // every reader has the descriptor
+      if (i == kTcEpiDone) count = kTcEpiWarps;                                      // every epilogue warp has written its rows
+      mbar_init(tc_bar(s, i), count);
+    }
     mbar_fence_init();
     *s.abort = 0;
   }
@@ -283,10 +301,10 @@ __device__ __forceinline__ float4 tc_split4(float4& x) {
 
 // Split the first `vecs` float4 of the landed raw chunk of `stage` into hi (in place) and lo
 // (lo buffer `lo`); the threads of warps 1-7.
-__device__ __forceinline__ void tc_split_stage(const TcState& s, int stage, int lo, int vecs) {
+__device__ __forceinline__ void tc_split_stage(const TcState& s, int stage, int lo, int vecs, int stride = 32 * kTcConvWarps) {
   float4* raw = reinterpret_cast<float4*>(s.base + kTcStageOffset + stage * kTcStageBytes);
   float4* low = reinterpret_cast<float4*>(s.base + kTcLoOffset + lo * kTcStageBytes);
-  for (int i = (int)threadIdx.x - 32; i < vecs; i += 32 * kTcConvWarps) {
+  for (int i = (int)threadIdx.x - 32; i < vecs; i += stride) {
     float4 x = raw[i];
     const float4 l = tc_split4(x);
     raw[i] = x;
@@ -341,7 +359,7 @@ __device__ inline bool tc_product(TcState& s, const TcMaps& maps, int a0, int b0
     int ok = 1;
     unsigned loads_pending = 0;  // stages whose TMA load was issued and not yet seen complete
     uint32_t pending_parity[kTcStages] = {};
-    bool c_pending = false, mma_issued = false;
+    bool c_pending = false, c_issued = false, mma_issued = false;
     // panels written by other CTAs of this launch were released to this thread by the flag
     // it acquired; the stages were last read by the previous unit's MMAs (waited for)
     fence_proxy_async_shared();
@@ -360,7 +378,7 @@ __device__ inline bool tc_product(TcState& s, const TcMaps& maps, int a0, int b0
       mbar_expect_tx(cbar, kTcCBytes);
       const uint64_t once = l2_policy_evict_first();
       for (int q = 0; q < 8; ++q) tma_load_3d(s.base_u + (uint32_t)q * kTcCChunkBytes, &maps.matrix, cx + 16 * q, cy, b, cbar, once);
-      c_pending = true;
+      c_pending = c_issued = true;
     };
     if (c_first) load_tile();
     for (int c = 0; c < kTcStages && c < nchunks && ok; ++c) {
@@ -369,7 +387,8 @@ __device__ inline bool tc_product(TcState& s, const TcMaps& maps, int a0, int b0
       if (g >= (uint32_t)kTcStages && !mbar_wait_or_abort(tc_bar(s, kTcEmpty + g % kTcStages), ((g - kTcStages) / kTcStages) & 1u, s.abort)) ok = 0;
       if (ok) issue(c, g);
     }
-    if (ok && !c_first) load_tile();
+    // an update unit's C tile goes behind the operand loads in the TMA queue (after the last
+    // refill): needed only by the epilogue, it would otherwise hold back chunks 4-7
     for (int c = 0; c < nchunks && ok; ++c) {
       const uint32_t g = g0 + c;
       const int stage = g % kTcStages;
@@ -399,8 +418,10 @@ __device__ inline bool tc_product(TcState& s, const TcMaps& maps, int a0, int b0
           break;
         }
         issue(c - 1 + kTcStages, gp + kTcStages);
+        if (c - 1 + kTcStages == nchunks - 1 && !c_issued) load_tile();
       }
     }
+    if (ok && !c_issued) load_tile();
     if (ok) {
       tc_commit(tc_bar(s, kTcAcc));
       mma_issued = false;
@@ -422,7 +443,8 @@ __device__ inline bool tc_product(TcState& s, const TcMaps& maps, int a0, int b0
     }
   } else if (tid >= 32) {
     // a row-panel unit reads its tile from the first chunk on
-    bool ok = b0 >= 0 || mbar_wait_or_abort(cbar, s.tile & 1u, s.abort);
+    // (decisions are made warp-uniform, so that a warp's lanes reach __syncwarp together)
+    bool ok = __all_sync(0xffffffffu, b0 >= 0 || mbar_wait_or_abort(cbar, s.tile & 1u, s.abort));
     for (int c = 0; c < nchunks && ok; ++c) {
       const uint32_t g = g0 + c;
       const int stage = g % kTcStages;
@@ -433,6 +455,7 @@ __device__ inline bool tc_product(TcState& s, const TcMaps& maps, int a0, int b0
         const uint32_t gp = g - kTcLoBufs;
         ok = mbar_wait_or_abort(tc_bar(s, kTcEmpty + gp % kTcStages), (gp / kTcStages) & 1u, s.abort);
       }
+      ok = __all_sync(0xffffffffu, ok);
       if (!ok) break;
       const int lo = g % kTcLoBufs;
       if (b0 >= 0) {
