@@ -6,7 +6,8 @@
 //   D = A_lo B_hi + A_hi B_lo + A_hi B_hi      (FP32 accumulation in TMEM, ~2^-21 relative)
 // Operand chunks of kTcChunk k-rows arrive by TMA (cp.async.bulk.tensor) in the canonical
 // K-major no-swizzle layout through a ring of kTcStages raw stages.  Warps 1-7 split a landed
-// chunk: hi = rna_tf32(x) in place, lo = rna_tf32(x - hi) into one of kTcLoBufs lo buffers.
+// chunk: the TF32 MMA reads an FP32 word through its leading 19 bits, so the raw word serves as
+// hi = trunc_tf32(x), and lo = rna_tf32(x - hi) goes into one of kTcLoBufs lo buffers.
 // Thread 0 issues the loads and tcgen05.mma.cta_group::1.kind::tf32 (M = N = 128, K = 8
 // per instruction) into a 128-column TMEM accumulator, and commits to mbarriers that free
 // the stages.  So the panels cost 4 bytes per element in global memory and on the way into
@@ -267,16 +268,6 @@ struct TcMaps {
   CUtensorMap matrix;  // 3-D {np, np, batch} over the FP64 work matrices, box {16, 128, 1}
 };
 
-// x = hi + lo with hi = rna_tf32(x) and lo = rna_tf32(x - hi) (x - hi is exact in FP32)
-__device__ __forceinline__ void tc_split_value(float f, float& hi, float& lo) {
-  unsigned h, l;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(f));
-  const float rest = f - __uint_as_float(h);
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(rest));
-  hi = __uint_as_float(h);
-  lo = __uint_as_float(l);
-}
-
 // Issue the TMA loads of operand chunk `c` (k rows c * kTcChunk ..) into raw stage `stage`:
 // A from panel block a0 + c and, when b0 >= 0, B from panel block b0 + c (a row-panel unit
 // builds B itself); thread 0 only.
@@ -289,27 +280,23 @@ __device__ __forceinline__ void tc_issue_chunk(const TcState& s, const CUtensorM
   if (b0 >= 0) tma_load_3d(dst + kTcArrayBytes, split, 0, 0, b0 + c, full, keep);
 }
 
-// x <- hi, returns lo, component by component.
-__device__ __forceinline__ float4 tc_split4(float4& x) {
-  float4 l;
-  tc_split_value(x.x, x.x, l.x);
-  tc_split_value(x.y, x.y, l.y);
-  tc_split_value(x.z, x.z, l.z);
-  tc_split_value(x.w, x.w, l.w);
-  return l;
+// The TF32 MMA reads an FP32 operand word through its leading 19 bits (sign, exponent, 10
+// mantissa bits), so the word itself serves as hi = trunc_tf32(x), and only
+// lo = rna_tf32(x - trunc_tf32(x)) (the difference is exact in FP32) has to be written.
+__device__ __forceinline__ float tc_lo_value(float x) {
+  const float rest = x - __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
+  unsigned l;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(rest));
+  return __uint_as_float(l);
 }
+__device__ __forceinline__ float4 tc_lo4(const float4& x) { return make_float4(tc_lo_value(x.x), tc_lo_value(x.y), tc_lo_value(x.z), tc_lo_value(x.w)); }
 
-// Split the first `vecs` float4 of the landed raw chunk of `stage` into hi (in place) and lo
-// (lo buffer `lo`); the threads of warps 1-7.
+// Split the first `vecs` float4 of the landed raw chunk of `stage`: hi is the raw word (left in
+// place), lo goes to lo buffer `lo`; the converter threads (warps 1 .. from thread 32 on).
 __device__ __forceinline__ void tc_split_stage(const TcState& s, int stage, int lo, int vecs, int stride = 32 * kTcConvWarps) {
   float4* raw = reinterpret_cast<float4*>(s.base + kTcStageOffset + stage * kTcStageBytes);
   float4* low = reinterpret_cast<float4*>(s.base + kTcLoOffset + lo * kTcStageBytes);
-  for (int i = (int)threadIdx.x - 32; i < vecs; i += stride) {
-    float4 x = raw[i];
-    const float4 l = tc_split4(x);
-    raw[i] = x;
-    low[i] = l;
-  }
+  for (int i = (int)threadIdx.x - 32; i < vecs; i += stride) low[i] = tc_lo4(raw[i]);
 }
 
 // Element (k, n) of the FP64 tile in the C buffer, stored with rows k (`rows_k`) or rows n.
@@ -330,9 +317,8 @@ __device__ __forceinline__ void tc_build_cold_chunk(const TcState& s, int stage,
                            static_cast<float>(tc_c_at(s, rows_k, k + 3, n)));
     const int o = ((n >> 3) * 4 + j) * 32 + (n & 7) * 4;
     *reinterpret_cast<float4*>(out + o) = x;
-    const float4 l = tc_split4(x);
     *reinterpret_cast<float4*>(hi_b + o) = x;
-    *reinterpret_cast<float4*>(lo_b + o) = l;
+    *reinterpret_cast<float4*>(lo_b + o) = tc_lo4(x);
   }
 }
 
