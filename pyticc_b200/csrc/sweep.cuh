@@ -689,10 +689,12 @@ __device__ inline bool step_wait(const int* f0, const int* f1, int target, int* 
 // ---- streamed update phase of a tensor-core step ------------------------------------------------
 // Once a CTA of a reduced step has claimed its first trailing-update unit, it stops working unit
 // by unit and streams every further update unit it can claim through warp-specialised roles:
-//   thread 0   claims units, waits for their row-panel flags, keeps the operand ring full across
-//              unit boundaries (chunk g of the CTA in stage g % 4, as in tc_product) and issues
-//              the MMAs into TMEM accumulator j % 2 of unit j;
-//   warps 1-3  split the landed chunks into TF32 hi/lo;
+//   thread 0   claims units, waits for their row-panel flags and keeps the operand ring full
+//              across unit boundaries (chunk g of the CTA in stage g % 4, as in tc_product),
+//              refilling a stage as soon as its products are done;
+//   warps 1-2  split the landed chunks into TF32 hi/lo;
+//   thread 96  (warp 3) issues each unit's MMAs into TMEM accumulator j % 2 and never waits
+//              for a product to finish;
 //   warps 4-7  run the epilogues (one TMEM lane = one row each): C <- C - D in the C buffer, then
 //              their leader (thread 128) stores the tile by TMA and, once the store has read
 //              the buffer, loads the next unit's C tile into it.
@@ -739,11 +741,9 @@ __device__ inline bool tc_update_stream(TcState& s, const TcMaps& maps, int b0, 
   const uint32_t g0 = s.chunk, tile0 = s.tile;
   const uint32_t cbar = tc_bar(s, kTcCFull);
   if (tid == 0) {
-    // ---- producer and MMA issuer
+    // ---- producer: claims units and keeps the operand ring full
     int ok = 1, n_units = 0;
-    bool ended = false, mma_issued = false;
-    unsigned loads_pending = 0;  // stages whose TMA load was issued and not yet seen split
-    uint32_t pending_parity[kTcStages] = {};
+    uint32_t g_next = g0;  // next chunk to load
     TcUnitDesc units[kTcDescSlots];
     auto publish = [&](int j, int b, int ta, int tb) -> bool {
       // the slot's previous descriptor (unit j - kTcDescSlots) has been read by every role
@@ -755,12 +755,16 @@ __device__ inline bool tc_update_stream(TcState& s, const TcMaps& maps, int b0, 
       mbar_arrive(tc_bar(s, kTcDescFull + j % kTcDescSlots));
       return true;
     };
-    // claim units until unit j exists or the queue is empty
-    auto ensure = [&](int j) -> bool {
-      while (ok && !ended && n_units <= j) {
+    fence_proxy_async_shared();
+    fence_proxy_async_global();
+    units[0] = TcUnitDesc{b0, ta0, tb0, 0};
+    if (publish(0, b0, ta0, tb0)) n_units = 1;
+    else ok = 0;
+    while (ok) {
+      const int j = (int)((g_next - g0) / nchunks), c = (int)((g_next - g0) % nchunks);
+      if (j == n_units) {  // the next unit: claim it (or end the stream)
         const int u = atomicAdd(queue, 1);
         if (u >= total) {
-          ended = true;
           if (!publish(n_units, -1, 0, 0)) ok = 0;
           break;
         }
@@ -780,68 +784,66 @@ __device__ inline bool tc_update_stream(TcState& s, const TcMaps& maps, int b0, 
         }
         ++n_units;
       }
-      return ok && j < n_units;
-    };
-    // issue chunk g (unit (g - g0) / 8) if that unit exists; false if it does not or a wait gave up
-    auto issue = [&](uint32_t g) -> bool {
-      const int j = (int)((g - g0) / nchunks), c = (int)((g - g0) % nchunks);
-      if (!ensure(j)) return false;
-      const int stage = g % kTcStages;
-      if (g >= (uint32_t)kTcStages && !mbar_wait_or_abort(tc_bar(s, kTcEmpty + stage), ((g - kTcStages) / kTcStages) & 1u, s.abort)) {
+      // the MMAs that last read this stage (chunk g_next - kTcStages) have completed
+      const int stage = g_next % kTcStages;
+      if (g_next >= (uint32_t)kTcStages && !mbar_wait_or_abort(tc_bar(s, kTcEmpty + stage), ((g_next - kTcStages) / kTcStages) & 1u, s.abort)) {
         ok = 0;
-        return false;
+        break;
       }
       const TcUnitDesc& d = units[j % kTcDescSlots];
       tc_issue_chunk(s, &maps.split, tc_split_block(d.b, 0, s.nt, d.ta, 0), tc_split_block(d.b, 1, s.nt, d.tb, 0), c, stage);
-      loads_pending |= 1u << stage;
-      pending_parity[stage] = (g / kTcStages) & 1u;
-      return true;
-    };
-    fence_proxy_async_shared();
-    fence_proxy_async_global();
-    units[0] = TcUnitDesc{b0, ta0, tb0, 0};
-    if (publish(0, b0, ta0, tb0)) n_units = 1;
-    else ok = 0;
-    for (int k = 0; k < kTcStages && ok; ++k)
-      if (!issue(g0 + k)) break;
-    for (uint32_t g = g0; ok; ++g) {
-      const int j = (int)((g - g0) / nchunks), c = (int)((g - g0) % nchunks);
-      if (j >= n_units) break;  // the queue is empty: every claimed unit has been multiplied
-      const int stage = g % kTcStages;
-      if (!mbar_wait_or_abort(tc_bar(s, kTcConv + stage), (g / kTcStages) & 1u, s.abort)) {
-        ok = 0;
-        break;
-      }
-      loads_pending &= ~(1u << stage);
-      // accumulator j % 2 has been read out by the epilogue of unit j - 2
-      if (c == 0 && j >= 2 && !mbar_wait_or_abort(tc_bar(s, kTcAccEmpty + (j & 1)), ((j - 2) / 2) & 1u, s.abort)) {
-        ok = 0;
-        break;
-      }
-      tc_fence_after();
-      const uint32_t d_tmem = s.tmem + (uint32_t)((j & 1) * kBlock);
-      const uint32_t st = s.base_u + kTcStageOffset + (uint32_t)stage * kTcStageBytes;
-      const uint32_t lo = s.base_u + kTcLoOffset + (uint32_t)(g % kTcLoBufs) * kTcStageBytes;
-#pragma unroll
-      for (int kg = 0; kg < kTcChunk / 8; ++kg) {
-        const uint64_t a_hi = tc_desc(st, kg), a_lo = tc_desc(lo, kg);
-        const uint64_t b_hi = tc_desc(st + kTcArrayBytes, kg), b_lo = tc_desc(lo + kTcArrayBytes, kg);
-        tc_mma_tf32(d_tmem, a_lo, b_hi, (c > 0 || kg > 0) ? 1u : 0u);
-        tc_mma_tf32(d_tmem, a_hi, b_lo, 1u);
-        tc_mma_tf32(d_tmem, a_hi, b_hi, 1u);
-      }
-      mma_issued = true;
-      tc_commit(tc_bar(s, kTcEmpty + stage));
-      if (c == nchunks - 1) tc_commit(tc_bar(s, kTcAccFull + (j & 1)));
-      // refill: chunk g + 3 into the stage of chunk g - 1 (its MMAs precede this chunk's)
-      if (g >= g0 + 1) issue(g + kTcStages - 1);
+      ++g_next;
     }
     if (!ok) {
       *s.abort = 1;  // the other roles stop waiting
       if (atomicExch(abort_flag, 1) == 0) report_status(status, kDeviceStalled, -1, -1);
-      for (int st = 0; st < kTcStages; ++st)
-        if (loads_pending & (1u << st)) mbar_wait(tc_bar(s, kTcFull + st), pending_parity[st]);
-      if (mma_issued) {
+      // the last kTcStages loads issued land before the CTA moves on (earlier ones were
+      // waited for through their stages' empty phases)
+      for (uint32_t g = (g_next > g0 + kTcStages ? g_next - kTcStages : g0); g < g_next; ++g) mbar_wait(tc_bar(s, kTcFull + g % kTcStages), (g / kTcStages) & 1u);
+    }
+  } else if (tid == 32 * kTcMmaWarp) {
+    // ---- MMA issuer: unit j into TMEM accumulator j % 2, never waiting for a product
+    bool ok = true, mma_issued = false;
+    for (int j = 0; ok; ++j) {
+      if (!mbar_wait_or_abort(tc_bar(s, kTcDescFull + j % kTcDescSlots), (j / kTcDescSlots) & 1u, s.abort)) {
+        ok = false;
+        break;
+      }
+      const int b = tc_desc_slot(s, j)->b;
+      mbar_arrive(tc_bar(s, kTcDescEmpty + j % kTcDescSlots));
+      if (b < 0) break;
+      const uint32_t d_tmem = s.tmem + (uint32_t)((j & 1) * kBlock);
+      for (int c = 0; c < nchunks; ++c) {
+        const uint32_t g = g0 + (uint32_t)(j * nchunks + c);
+        const int stage = g % kTcStages;
+        if (!mbar_wait_or_abort(tc_bar(s, kTcConv + stage), (g / kTcStages) & 1u, s.abort)) {
+          ok = false;
+          break;
+        }
+        // accumulator j % 2 has been read out by the epilogue of unit j - 2
+        if (c == 0 && j >= 2 && !mbar_wait_or_abort(tc_bar(s, kTcAccEmpty + (j & 1)), ((j - 2) / 2) & 1u, s.abort)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t st = s.base_u + kTcStageOffset + (uint32_t)stage * kTcStageBytes;
+        const uint32_t lo = s.base_u + kTcLoOffset + (uint32_t)(g % kTcLoBufs) * kTcStageBytes;
+#pragma unroll
+        for (int kg = 0; kg < kTcChunk / 8; ++kg) {
+          const uint64_t a_hi = tc_desc(st, kg), a_lo = tc_desc(lo, kg);
+          const uint64_t b_hi = tc_desc(st + kTcArrayBytes, kg), b_lo = tc_desc(lo + kTcArrayBytes, kg);
+          tc_mma_tf32(d_tmem, a_lo, b_hi, (c > 0 || kg > 0) ? 1u : 0u);
+          tc_mma_tf32(d_tmem, a_hi, b_lo, 1u);
+          tc_mma_tf32(d_tmem, a_hi, b_hi, 1u);
+        }
+        mma_issued = true;
+        tc_commit(tc_bar(s, kTcEmpty + stage));
+        if (c == nchunks - 1) tc_commit(tc_bar(s, kTcAccFull + (j & 1)));
+      }
+    }
+    if (!ok) {
+      *s.abort = 1;
+      if (mma_issued) {  // the products land before the CTA moves on or frees TMEM
         tc_commit(tc_bar(s, kTcDrain));
         mbar_wait(tc_bar(s, kTcDrain), 0u);
       }
@@ -868,7 +870,7 @@ __device__ inline bool tc_update_stream(TcState& s, const TcMaps& maps, int b0, 
           ok = false;
           break;
         }
-        tc_split_stage(s, stage, g % kTcLoBufs, kTcStageBytes / 16, 32 * kTcStreamConvWarps);
+        tc_split_stage_all<32 * kTcStreamConvWarps>(s, stage, g % kTcLoBufs);
         fence_proxy_async_shared();  // read next by the tensor core
         __syncwarp();
         // the conversion barrier counts kTcConvWarps warp arrivals: warp 1 stands in for the rest
@@ -876,12 +878,22 @@ __device__ inline bool tc_update_stream(TcState& s, const TcMaps& maps, int b0, 
       }
     }
     if (!ok) *s.abort = 1;
-  } else if (warp > kTcStreamConvWarps) {
-    // ---- warps 4-7: epilogues; thread 128 also moves the C tiles
-    const bool leader = tid == 32 * (kTcStreamConvWarps + 1);
+  } else if (warp > kTcMmaWarp) {
+    // ---- warps 4-7: epilogues, in two column halves of the C buffer; thread 128 moves the C
+    // tiles half by half, so that the next tile's first half loads while this tile's second
+    // half is still being formed and stored
+    const bool leader = tid == 32 * (kTcMmaWarp + 1);
     const int r = 32 * (warp & 3) + lane;  // TMEM lane = tile row of this thread
-    bool ok = true, c_pending = false;
-    uint32_t c_phase = 0;
+    const uint32_t cbar_hi = tc_bar(s, kTcCFullHi);
+    bool ok = true;
+    unsigned c_pending = 0;  // halves whose load this thread issued and no epilogue has waited for
+    uint32_t c_phase[2] = {0, 0};
+    auto load_half = [&](const TcUnitDesc& d, int h, uint32_t bar) {
+      fence_proxy_async_shared();
+      mbar_expect_tx(bar, kTcCBytes / 2);
+      const uint64_t once = l2_policy_evict_first();
+      for (int q = 4 * h; q < 4 * h + 4; ++q) tma_load_3d(s.base_u + (uint32_t)q * kTcCChunkBytes, &maps.matrix, d.tb * kBlock + 16 * q, d.ta * kBlock, d.b, bar, once);
+    };
     for (int j = 0; ok; ++j) {
       ok = __all_sync(0xffffffffu, mbar_wait_or_abort(tc_bar(s, kTcDescFull + j % kTcDescSlots), (j / kTcDescSlots) & 1u, s.abort));
       if (!ok) break;
@@ -892,76 +904,99 @@ __device__ inline bool tc_update_stream(TcState& s, const TcMaps& maps, int b0, 
       __syncwarp();
       if (lane == 0) mbar_arrive(tc_bar(s, kTcDescEmpty + j % kTcDescSlots));
       if (d.b < 0) break;
+      const uint32_t ph_lo = (tile0 + (uint32_t)j) & 1u, ph_hi = (uint32_t)j & 1u;
       if (leader && j == 0) {  // the C buffer is free: earlier units of this CTA left no store pending
-        tc_stream_load_c(s, maps, d);
-        c_pending = true;
-        c_phase = tile0 & 1u;
+        load_half(d, 0, cbar);
+        load_half(d, 1, cbar_hi);
+        c_pending = 3u;
+        c_phase[0] = ph_lo;
+        c_phase[1] = ph_hi;
       }
+      const bool diagonal = d.ta == d.tb;
+      // a diagonal tile's mirror writes reach the second half from the first
       bool w = mbar_wait_or_abort(tc_bar(s, kTcAccFull + (j & 1)), (j / 2) & 1u, s.abort);
-      if (w) w = mbar_wait_or_abort(cbar, (tile0 + (uint32_t)j) & 1u, s.abort);
+      if (w) w = mbar_wait_or_abort(cbar, ph_lo, s.abort);
+      if (w && diagonal) w = mbar_wait_or_abort(cbar_hi, ph_hi, s.abort);
       if (!__all_sync(0xffffffffu, w)) {
         ok = false;
         break;
       }
-      if (leader) c_pending = false;
       tc_fence_after();
       const uint32_t row_tmem = s.tmem + (uint32_t)((j & 1) * kBlock) + ((uint32_t)(32 * (warp & 3)) << 16);
-      const bool diagonal = d.ta == d.tb;
+      for (int h = 0; h < 2 && ok; ++h) {
+        if (h == 1 && !diagonal && !__all_sync(0xffffffffu, mbar_wait_or_abort(cbar_hi, ph_hi, s.abort))) {
+          ok = false;
+          break;
+        }
+        if (h == 1) tc_fence_after();
 #pragma unroll 1
-      for (int q = 0; q < kBlock / 16; ++q) {
-        const int col = 16 * q;
-        float dv[16];
-        tc_ld_16(row_tmem + (uint32_t)col, dv);
-        if (!diagonal) {
+        for (int q = 0; q < 2; ++q) {
+          const int col = 64 * h + 32 * q;
+          float dv[32];
+          tc_ld_32(row_tmem + (uint32_t)col, dv);
+          if (!diagonal) {
+            double2 v[16];
 #pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            double2* p = reinterpret_cast<double2*>(s.base + tc_c_offset(r, col + 2 * u));
-            double2 v = *p;
-            v.x -= (double)dv[2 * u];
-            v.y -= (double)dv[2 * u + 1];
-            *p = v;
-          }
-        } else if (col <= r) {
-          // a diagonal tile keeps its lower half and mirrors it: row r writes (r, n) and
-          // (n, r) for n <= r; the upper elements of row r are written by the rows below
+            for (int u = 0; u < 16; ++u) v[u] = *reinterpret_cast<const double2*>(s.base + tc_c_offset(r, col + 2 * u));
 #pragma unroll
-          for (int u = 0; u < 16; ++u) {
-            const int n = col + u;
-            if (n <= r) {
-              double* p = reinterpret_cast<double*>(s.base + tc_c_offset(r, n));
-              const double v = *p - (double)dv[u];
-              *p = v;
-              *reinterpret_cast<double*>(s.base + tc_c_offset(n, r)) = v;
+            for (int u = 0; u < 16; ++u) {
+              v[u].x -= (double)dv[2 * u];
+              v[u].y -= (double)dv[2 * u + 1];
+              *reinterpret_cast<double2*>(s.base + tc_c_offset(r, col + 2 * u)) = v[u];
+            }
+          } else if (col <= r) {
+            // a diagonal tile keeps its lower half and mirrors it: row r writes (r, n) and
+            // (n, r) for n <= r; the upper elements of row r are written by the rows below
+#pragma unroll
+            for (int u = 0; u < 32; ++u) {
+              const int n = col + u;
+              if (n <= r) {
+                double* p = reinterpret_cast<double*>(s.base + tc_c_offset(r, n));
+                const double v = *p - (double)dv[u];
+                *p = v;
+                *reinterpret_cast<double*>(s.base + tc_c_offset(n, r)) = v;
+              }
             }
           }
         }
-      }
-      tc_fence_before();
-      fence_proxy_async_shared();  // the rows are read next by the TMA store
-      __syncwarp();
-      if (lane == 0) {
-        mbar_arrive(tc_bar(s, kTcAccEmpty + (j & 1)));
-        mbar_arrive(tc_bar(s, kTcEpiDone));
-      }
-      if (leader) {
-        // every epilogue warp has written its rows: store the tile, then load the next one
-        bool l = mbar_wait_or_abort(tc_bar(s, kTcEpiDone), (uint32_t)j & 1u, s.abort);
-        if (l) {
-          const uint64_t once = l2_policy_evict_first();
-          for (int q = 0; q < 8; ++q) tma_store_3d(&maps.matrix, s.base_u + (uint32_t)q * kTcCChunkBytes, d.tb * kBlock + 16 * q, d.ta * kBlock, d.b, once);
-          bulk_commit();
-          l = mbar_wait_or_abort(tc_bar(s, kTcDescFull + (j + 1) % kTcDescSlots), ((j + 1) / kTcDescSlots) & 1u, s.abort);
+        if (h == 1) tc_fence_before();
+        fence_proxy_async_shared();  // the rows are read next by the TMA store
+        __syncwarp();
+        if (lane == 0) {
+          if (h == 1) mbar_arrive(tc_bar(s, kTcAccEmpty + (j & 1)));
+          mbar_arrive(tc_bar(s, h == 0 ? kTcEpiDone : kTcEpiDoneHi));
         }
+        if (leader) {
+          // every epilogue warp has written this half (a diagonal tile's first half is final
+          // once every row has done its first half; its second half, once every row is done)
+          bool l = mbar_wait_or_abort(tc_bar(s, h == 0 ? kTcEpiDone : kTcEpiDoneHi), (uint32_t)j & 1u, s.abort);
+          if (l) {
+            c_pending &= ~(1u << h);
+            const uint64_t once = l2_policy_evict_first();
+            for (int q = 4 * h; q < 4 * h + 4; ++q) tma_store_3d(&maps.matrix, s.base_u + (uint32_t)q * kTcCChunkBytes, d.tb * kBlock + 16 * q, d.ta * kBlock, d.b, once);
+            bulk_commit();
+          }
+          ok = l;
+        }
+        ok = __all_sync(0xffffffffu, ok);
+      }
+      if (!ok) break;
+      if (leader) {
+        // the next unit's C tile, half by half as this tile's stores read the buffer out
+        bool l = mbar_wait_or_abort(tc_bar(s, kTcDescFull + (j + 1) % kTcDescSlots), ((j + 1) / kTcDescSlots) & 1u, s.abort);
         if (l) {
           TcUnitDesc nd;
           nd.b = tc_desc_slot(s, j + 1)->b;
           nd.ta = tc_desc_slot(s, j + 1)->ta;
           nd.tb = tc_desc_slot(s, j + 1)->tb;
           if (nd.b >= 0) {
-            bulk_wait_read_all();  // the store has read the buffer
-            tc_stream_load_c(s, maps, nd);
-            c_pending = true;
-            c_phase = (tile0 + (uint32_t)j + 1) & 1u;
+            asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");  // the first half's store
+            load_half(nd, 0, cbar);
+            bulk_wait_read_all();
+            load_half(nd, 1, cbar_hi);
+            c_pending = 3u;
+            c_phase[0] = (tile0 + (uint32_t)j + 1) & 1u;
+            c_phase[1] = (uint32_t)(j + 1) & 1u;
           }
         }
         ok = l;
@@ -970,7 +1005,8 @@ __device__ inline bool tc_update_stream(TcState& s, const TcMaps& maps, int b0, 
     }
     if (leader) {
       bulk_wait_all();  // this thread's stores are complete before the CTA moves on
-      if (c_pending) mbar_wait(cbar, c_phase);
+      if (c_pending & 1u) mbar_wait(cbar, c_phase[0]);
+      if (c_pending & 2u) mbar_wait(cbar_hi, c_phase[1]);
     }
     if (!ok) *s.abort = 1;
   }

@@ -3,11 +3,11 @@
 // One unit computes C <- C - A^T B for a 128 x 128 FP64 tile C of a work matrix, with
 // A = the old pivot rows (cold, 128 x 128 block of columns ta) and B = U = P^-1 cold
 // (columns tb), both given as FP32 panels and split in shared memory as x = hi + lo in TF32:
-//   D = A_lo B_hi + A_hi B_lo + A_hi B_hi      (FP32 accumulation in TMEM, ~2^-21 relative)
+//   D = A_lo B_hi + A_hi B_lo + A_hi B_hi      (FP32 accumulation in TMEM, ~2^-20 relative)
 // Operand chunks of kTcChunk k-rows arrive by TMA (cp.async.bulk.tensor) in the canonical
 // K-major no-swizzle layout through a ring of kTcStages raw stages.  Warps 1-7 split a landed
 // chunk: the TF32 MMA reads an FP32 word through its leading 19 bits, so the raw word serves as
-// hi = trunc_tf32(x), and lo = rna_tf32(x - hi) goes into one of kTcLoBufs lo buffers.
+// hi = trunc_tf32(x), and lo = x - hi goes into one of kTcLoBufs lo buffers.
 // Thread 0 issues the loads and tcgen05.mma.cta_group::1.kind::tf32 (M = N = 128, K = 8
 // per instruction) into a 128-column TMEM accumulator, and commits to mbarriers that free
 // the stages.  So the panels cost 4 bytes per element in global memory and on the way into
@@ -64,12 +64,14 @@ constexpr int kTcFull = 0, kTcEmpty = kTcStages, kTcConv = 2 * kTcStages, kTcAcc
 // descriptors, and the epilogue warps' hand-over of a finished C tile to its store
 constexpr int kTcDescSlots = 4;
 constexpr int kTcAccFull = 3 * kTcStages + 3, kTcAccEmpty = kTcAccFull + 2, kTcDescFull = kTcAccEmpty + 2, kTcDescEmpty = kTcDescFull + kTcDescSlots, kTcEpiDone = kTcDescEmpty + kTcDescSlots;
-constexpr int kTcBarriers = kTcEpiDone + 1;
+constexpr int kTcEpiDoneHi = kTcEpiDone + 1, kTcCFullHi = kTcEpiDone + 2;  // the C buffer's second column half
+constexpr int kTcBarriers = kTcEpiDone + 3;
 constexpr int kTcEpiWarps = 4;     // warps 4-7 (TMEM lanes 0-127) in the streamed phase
-constexpr int kTcStreamConvWarps = 3;  // warps 1-3 split the chunks there
+constexpr int kTcStreamConvWarps = 2;  // warps 1-2 split the chunks there
+constexpr int kTcMmaWarp = 3;           // and lane 0 of warp 3 issues the MMAs
 static_assert(kTcStages % kTcLoBufs == 0, "a stage must always pair with the same lo buffer");
 static_assert(kGemmThreads == 32 * (kTcConvWarps + 1), "the units run with thread 0 issuing and warps 1-7 converting");
-static_assert(kTcStreamConvWarps + kTcEpiWarps + 1 == kGemmThreads / 32 && kTcEpiWarps == 4, "the streamed phase: warp 0 issues, then converter warps, then four epilogue warps (TMEM lanes 0-127)");
+static_assert(kTcMmaWarp == kTcStreamConvWarps + 1 && kTcMmaWarp + 1 + kTcEpiWarps == kGemmThreads / 32 && kTcEpiWarps == 4, "the streamed phase: warp 0 loads, then converter warps, the MMA warp, four epilogue warps (TMEM lanes 0-127)");
 constexpr int kTcTmemSlotOffset = kTcBarOffset + 8 * kTcBarriers;   // TMEM address, then the abort flag at + 8
 constexpr int kTcDescOffset = kTcTmemSlotOffset + 16;                // kTcDescSlots x 16 bytes
 constexpr int kTcRegionBytes = kTcDescOffset + 16 * kTcDescSlots;
@@ -174,6 +176,20 @@ __device__ __forceinline__ void tc_mma_tf32(uint32_t d_tmem, uint64_t adesc, uin
 __device__ __forceinline__ void tc_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
+__device__ __forceinline__ void tc_ld_32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, "
+      "%27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
 __device__ __forceinline__ void tc_ld_16(uint32_t taddr, float (&v)[16]) {
   uint32_t r[16];
   asm volatile(
@@ -237,8 +253,8 @@ __device__ inline void tc_setup(TcState& s, void* dynamic_smem, int np) {
       uint32_t count = 1;
       if (i >= kTcConv && i < kTcConv + kTcStages) count = kTcConvWarps;            // a warp-level arrival of every converter warp
       if (i >= kTcAccEmpty && i < kTcAccEmpty + 2) count = kTcEpiWarps;             // every epilogue warp has read the accumulator
-      if (i >= kTcDescEmpty && i < kTcDescEmpty + kTcDescSlots) count = kTcStreamConvWarps + kTcEpiWarps;  // every reader has the descriptor
-      if (i == kTcEpiDone) count = kTcEpiWarps;                                      // every epilogue warp has written its rows
+      if (i >= kTcDescEmpty && i < kTcDescEmpty + kTcDescSlots) count = kTcStreamConvWarps + 1 + kTcEpiWarps;  // every reader has the descriptor
+      if (i == kTcEpiDone || i == kTcEpiDoneHi) count = kTcEpiWarps;                 // every epilogue warp has written its rows
       mbar_init(tc_bar(s, i), count);
     }
     mbar_fence_init();
@@ -281,14 +297,10 @@ __device__ __forceinline__ void tc_issue_chunk(const TcState& s, const CUtensorM
 }
 
 // The TF32 MMA reads an FP32 operand word through its leading 19 bits (sign, exponent, 10
-// mantissa bits), so the word itself serves as hi = trunc_tf32(x), and only
-// lo = rna_tf32(x - trunc_tf32(x)) (the difference is exact in FP32) has to be written.
-__device__ __forceinline__ float tc_lo_value(float x) {
-  const float rest = x - __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
-  unsigned l;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(rest));
-  return __uint_as_float(l);
-}
+// mantissa bits), so the word itself serves as hi = trunc_tf32(x), and lo = x - hi (exact in
+// FP32) is written as it is: the MMA reads its leading 19 bits in turn, so hi + trunc_tf32(lo)
+// carries x to 2^-20 relative.
+__device__ __forceinline__ float tc_lo_value(float x) { return x - __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
 __device__ __forceinline__ float4 tc_lo4(const float4& x) { return make_float4(tc_lo_value(x.x), tc_lo_value(x.y), tc_lo_value(x.z), tc_lo_value(x.w)); }
 
 // Split the first `vecs` float4 of the landed raw chunk of `stage`: hi is the raw word (left in
@@ -296,7 +308,25 @@ __device__ __forceinline__ float4 tc_lo4(const float4& x) { return make_float4(t
 __device__ __forceinline__ void tc_split_stage(const TcState& s, int stage, int lo, int vecs, int stride = 32 * kTcConvWarps) {
   float4* raw = reinterpret_cast<float4*>(s.base + kTcStageOffset + stage * kTcStageBytes);
   float4* low = reinterpret_cast<float4*>(s.base + kTcLoOffset + lo * kTcStageBytes);
+#pragma unroll 4
   for (int i = (int)threadIdx.x - 32; i < vecs; i += stride) low[i] = tc_lo4(raw[i]);
+}
+
+// The same for a whole 16 KB stage with kThreads converter threads (from thread 32 on), each
+// taking kStageVecs / kThreads float4: all loads first, then the differences and stores, so
+// that one shared-memory latency covers the chunk.
+template <int kThreads>
+__device__ __forceinline__ void tc_split_stage_all(const TcState& s, int stage, int lo) {
+  constexpr int kVecs = kTcStageBytes / 16, kPer = kVecs / kThreads;
+  static_assert(kVecs % kThreads == 0, "every converter thread takes the same number of float4");
+  const float4* raw = reinterpret_cast<const float4*>(s.base + kTcStageOffset + stage * kTcStageBytes);
+  float4* low = reinterpret_cast<float4*>(s.base + kTcLoOffset + lo * kTcStageBytes);
+  const int i0 = (int)threadIdx.x - 32;
+  float4 x[kPer];
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) x[k] = raw[i0 + k * kThreads];
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) low[i0 + k * kThreads] = tc_lo4(x[k]);
 }
 
 // Element (k, n) of the FP64 tile in the C buffer, stored with rows k (`rows_k`) or rows n.
