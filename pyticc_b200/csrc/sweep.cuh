@@ -39,92 +39,89 @@ static_assert(kPivotAuxBytes <= size_t(kUpdStageDoubles) * sizeof(double), "pivo
 
 // Gauss-Jordan exchange of a 64x64 sub-block S (row stride Ld) with partial
 // pivoting over its rows, by the kPivotThreads threads of the CTA; writes the inverse in
-// natural order to X (row stride kSub).  Thread t owns column t % 64 and every 4th row
-// from t / 64, so a step updates 16 elements per thread branch-free, the pivot row and
-// column are broadcast reads and the next pivot search runs in the 4 owners of the next
-// column.  Two barriers per step.  Returns true if a pivot was zero or non-finite.
+// natural order to X (row stride kSub).  Thread t holds row t % 64, columns 16 (t / 64) ..
+// + 15 of the block in registers for the whole exchange: a step publishes only the pivot
+// row (its 4 owners) and the pivot column (one value per row) through shared memory, and the
+// next pivot is found by a warp-shuffle maximum over the 32 rows of each of the 2 warps that
+// hold the next column.  Pivot choice: largest magnitude among the rows not yet used, the
+// smallest row on ties, a NaN ranking as zero.  Two barriers per step.  Returns true if a
+// pivot was zero or non-finite.
 template <int Ld = kPivotLd>
 __device__ inline bool gauss_jordan_sub(double* S, double* X, double* aux) {
-  constexpr int G = kPivotThreads / kSub;
-  constexpr int RPT = kSub / G;
+  static_assert(kPivotThreads == 4 * kSub, "one thread per (row, 16-column group)");
   double* prow = aux;
   double* pcol = aux + kSub;
   double* cand_val = aux + 2 * kSub;
   int* cand_row = reinterpret_cast<int*>(cand_val + 4);
   int* perm = cand_row + 4;
-  const int t = threadIdx.x, c = t & (kSub - 1), g = t / kSub;
-  unsigned used = 0u;
-  bool singular = false;
-  if (c == 0) {
-    double best = -1.0;
-    int row = kSub;
+  const int t = threadIdx.x, r = t & (kSub - 1), cg = t / kSub, lane = t & 31, half = r >> 5;
+  double v[16];
 #pragma unroll
-    for (int i = 0; i < RPT; ++i) {
-      const double m = fabs(S[(g + G * i) * Ld]);
-      const double v = (m >= 0.0) ? m : 0.0;  // a NaN entry ranks as zero, then flags the pivot
-      if (v > best) {
-        best = v;
-        row = g + G * i;
+  for (int i = 0; i < 16; ++i) v[i] = S[r * Ld + 16 * cg + i];
+  bool row_used = false, singular = false;
+  // the largest candidate of this warp's 32 rows (a used row ranks -1, a NaN 0) to slot `half`
+  auto candidate = [&](double m, bool excluded) {
+    double w = excluded ? -1.0 : (m >= 0.0 ? m : 0.0);
+    int row = r;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double w2 = __shfl_xor_sync(0xffffffffu, w, off);
+      const int r2 = __shfl_xor_sync(0xffffffffu, row, off);
+      if (w2 > w || (w2 == w && r2 < row)) {
+        w = w2;
+        row = r2;
       }
     }
-    cand_val[g] = best;
-    cand_row[g] = row;
-  }
+    if (lane == 0) {
+      cand_val[half] = w;
+      cand_row[half] = row;
+    }
+  };
+  if (cg == 0) candidate(fabs(v[0]), false);
   __syncthreads();
-  for (int j = 0; j < kSub; ++j) {
-    double best = -1.0;
-    int p = kSub;
+#pragma unroll 1
+  for (int blk = 0; blk < kSub / 16; ++blk) {
 #pragma unroll
-    for (int q = 0; q < G; ++q) {
-      const double v = cand_val[q];
-      const int r = cand_row[q];
-      if (v > best || (v == best && r < p)) {
-        best = v;
-        p = r;
+    for (int jj = 0; jj < 16; ++jj) {
+      const int j = 16 * blk + jj;
+      double best = cand_val[0];
+      int p = cand_row[0];
+      const double b1 = cand_val[1];
+      const int p1 = cand_row[1];
+      if (b1 > best || (b1 == best && p1 < p)) {
+        best = b1;
+        p = p1;
       }
-    }
-    double a = S[p * Ld + j];
-    if (!(fabs(a) > 0.0) || !isfinite(a)) {
-      singular = true;
-      a = 1.0;
-    }
-    const double inv_a = 1.0 / a;
-    if (g == 0) prow[c] = S[p * Ld + c];
-    if (g == G - 1) pcol[c] = S[c * Ld + j];
-    if (t == 0) perm[j] = p;
-    if (p % G == g) used |= 1u << (p / G);
-    __syncthreads();
-    const double pr = prow[c] * inv_a;
-    double pc[RPT], v[RPT];
+      const bool mine = r == p;
+      if (mine) {
 #pragma unroll
-    for (int u = 0; u < RPT; ++u) pc[u] = pcol[g + G * u];
-#pragma unroll
-    for (int u = 0; u < RPT; ++u) v[u] = S[(g + G * u) * Ld + c];
-    const int mine = (p % G == g) ? p / G : -1;
-#pragma unroll
-    for (int u = 0; u < RPT; ++u) {
-      const double w = (c == j) ? pc[u] * inv_a : v[u] - pc[u] * pr;
-      v[u] = (u == mine) ? ((c == j) ? inv_a : -pr) : w;
-    }
-#pragma unroll
-    for (int u = 0; u < RPT; ++u) S[(g + G * u) * Ld + c] = v[u];
-    if (c == j + 1) {
-      double b2 = -1.0;
-      int row = kSub;
-#pragma unroll
-      for (int u = 0; u < RPT; ++u) {
-        const double m = fabs(v[u]);
-        const double w = ((used >> u) & 1u) ? -1.0 : (m >= 0.0 ? m : 0.0);
-        if (w > b2) {
-          b2 = w;
-          row = g + G * u;
-        }
+        for (int i = 0; i < 16; ++i) prow[16 * cg + i] = v[i];
+        row_used = true;
       }
-      cand_val[g] = b2;
-      cand_row[g] = row;
+      if (cg == blk) pcol[r] = v[jj];
+      if (t == 0) perm[j] = p;
+      __syncthreads();
+      double a = prow[j];
+      if (!(fabs(a) > 0.0) || !isfinite(a)) {
+        singular = true;
+        a = 1.0;
+      }
+      const double inv_a = 1.0 / a;
+      const double pc = pcol[r];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int c = 16 * cg + i;
+        const double pr = prow[c] * inv_a;
+        const double w = (c == j) ? pc * inv_a : v[i] - pc * pr;
+        v[i] = mine ? ((c == j) ? inv_a : -pr) : w;
+      }
+      if (j + 1 < kSub && cg == (j + 1) / 16) candidate(fabs(v[(jj + 1) & 15]), row_used);
+      __syncthreads();
     }
-    __syncthreads();
   }
+#pragma unroll
+  for (int i = 0; i < 16; ++i) S[r * Ld + 16 * cg + i] = v[i];
+  __syncthreads();
   // inverse element (j, perm[c]) sits at exchange slot (perm[j], c)
   int* iperm = reinterpret_cast<int*>(prow);
   if (t < kSub) iperm[perm[t]] = t;
@@ -708,15 +705,26 @@ struct TcUnitDesc {
 
 __device__ __forceinline__ volatile TcUnitDesc* tc_desc_slot(const TcState& s, int j) { return reinterpret_cast<volatile TcUnitDesc*>(s.base + kTcDescOffset) + (j % kTcDescSlots); }
 
-// Bounded poll of two row-panel flags by one thread (thread 0 of the streaming CTA).
+__device__ __forceinline__ int load_relaxed(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Bounded poll of two row-panel flags by one thread (thread 0 of the streaming CTA): both
+// loads in flight together, then one acquire fence once both are set.
 __device__ inline bool tc_flags_ready(const int* fa, const int* fb, int target, int* abort_flag, int* status, int b) {
   const long long limit = g_step_poll_limit;
   for (long long it = 0;; ++it) {
+    const int va = load_relaxed(fa), vb = load_relaxed(fb);
+    if (va >= target && vb >= target) {
+      asm volatile("fence.acq_rel.gpu;" ::: "memory");
+      return true;
+    }
     if (it >= limit || load_acquire(abort_flag) != 0) {
       if (atomicExch(abort_flag, 1) == 0) report_status(status, kDeviceStalled, b, target);
       return false;
     }
-    if (load_acquire(fa) >= target && load_acquire(fb) >= target) return true;
     __nanosleep(128);
   }
 }
@@ -745,6 +753,10 @@ __device__ inline bool tc_update_stream(TcState& s, const TcMaps& maps, int b0, 
     int ok = 1, n_units = 0;
     uint32_t g_next = g0;  // next chunk to load
     TcUnitDesc units[kTcDescSlots];
+    // units are claimed two at a time; the row-panel flags already seen set for the current
+    // matrix are remembered (bit ct of `seen` for matrix seen_b)
+    int claim_next = 0, claim_left = 0, seen_b = -1;
+    uint32_t seen = 0;
     auto publish = [&](int j, int b, int ta, int tb) -> bool {
       // the slot's previous descriptor (unit j - kTcDescSlots) has been read by every role
       if (j >= kTcDescSlots && !mbar_wait_or_abort(tc_bar(s, kTcDescEmpty + j % kTcDescSlots), ((j - kTcDescSlots) / kTcDescSlots) & 1u, s.abort)) return false;
@@ -763,7 +775,12 @@ __device__ inline bool tc_update_stream(TcState& s, const TcMaps& maps, int b0, 
     while (ok) {
       const int j = (int)((g_next - g0) / nchunks), c = (int)((g_next - g0) % nchunks);
       if (j == n_units) {  // the next unit: claim it (or end the stream)
-        const int u = atomicAdd(queue, 1);
+        if (claim_left == 0) {
+          claim_next = atomicAdd(queue, 2);
+          claim_left = 2;
+        }
+        const int u = claim_next++;
+        --claim_left;
         if (u >= total) {
           if (!publish(n_units, -1, 0, 0)) ok = 0;
           break;
@@ -772,11 +789,19 @@ __device__ inline bool tc_update_stream(TcState& s, const TcMaps& maps, int b0, 
         update_tile_of<true>(u - first_update, per, t, kb, b, ta, tb);
         if (fuse_next && ta == kb + 1 && tb == kb + 1) continue;  // the pivot unit's tile
         const int* fl = ints + b * kStepIntsPerMatrix + kStepFlagOffset;
-        if (!tc_flags_ready(fl + ta, fl + tb, kb + 1, abort_flag, status, b)) {
-          ok = 0;
-          break;
+        if (b != seen_b) {
+          seen_b = b;
+          seen = 0;
         }
-        fence_proxy_async_global();  // the released panels are read next by TMA
+        const uint32_t need = (1u << ta) | (1u << tb);
+        if ((seen & need) != need) {
+          if (!tc_flags_ready(fl + ta, fl + tb, kb + 1, abort_flag, status, b)) {
+            ok = 0;
+            break;
+          }
+          seen |= need;
+          fence_proxy_async_global();  // the released panels are read next by TMA
+        }
         units[n_units % kTcDescSlots] = TcUnitDesc{b, ta, tb, 0};
         if (!publish(n_units, b, ta, tb)) {
           ok = 0;
