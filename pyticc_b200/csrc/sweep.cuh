@@ -42,9 +42,9 @@ static_assert(kPivotAuxBytes <= size_t(kUpdStageDoubles) * sizeof(double), "pivo
 // natural order to X (row stride kSub).  Thread t holds row t % 64, columns 16 (t / 64) ..
 // + 15 of the block in registers for the whole exchange: a step publishes only the pivot
 // row (its 4 owners) and the pivot column (one value per row) through shared memory, and the
-// next pivot is found by a warp-shuffle maximum over the 32 rows of each of the 2 warps that
-// hold the next column.  Pivot choice: largest magnitude among the rows not yet used, the
-// smallest row on ties, a NaN ranking as zero.  Two barriers per step.  Returns true if a
+// next pivot is found as the maximum over the 32 rows of each of the 2 warps that
+// hold the next column (warp reductions on a rank key).  Pivot choice: largest magnitude among
+// the rows not yet used, the smallest row on ties, a NaN ranking as zero.  Two barriers per step.  Returns true if a
 // pivot was zero or non-finite.
 template <int Ld = kPivotLd>
 __device__ inline bool gauss_jordan_sub(double* S, double* X, double* aux) {
@@ -59,22 +59,19 @@ __device__ inline bool gauss_jordan_sub(double* S, double* X, double* aux) {
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = S[r * Ld + 16 * cg + i];
   bool row_used = false, singular = false;
-  // the largest candidate of this warp's 32 rows (a used row ranks -1, a NaN 0) to slot `half`
+  // this warp's best row for the next pivot to slot `half`.  Rank: 0 for a used row, else 1 +
+  // the bit pattern of the magnitude (a NaN as zero), which orders like the magnitude; the
+  // largest rank wins, the smallest row on ties: three warp reductions instead of shuffles.
+  unsigned long long* cand_key = reinterpret_cast<unsigned long long*>(cand_val);
   auto candidate = [&](double m, bool excluded) {
-    double w = excluded ? -1.0 : (m >= 0.0 ? m : 0.0);
-    int row = r;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const double w2 = __shfl_xor_sync(0xffffffffu, w, off);
-      const int r2 = __shfl_xor_sync(0xffffffffu, row, off);
-      if (w2 > w || (w2 == w && r2 < row)) {
-        w = w2;
-        row = r2;
-      }
-    }
+    const unsigned long long key = excluded ? 0ull : 1ull + (unsigned long long)__double_as_longlong(m >= 0.0 ? m : 0.0);
+    const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+    const unsigned hmax = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned lmax = __reduce_max_sync(0xffffffffu, hi == hmax ? lo : 0u);
+    const unsigned rmin = __reduce_min_sync(0xffffffffu, (hi == hmax && lo == lmax) ? (unsigned)r : 0xffffffffu);
     if (lane == 0) {
-      cand_val[half] = w;
-      cand_row[half] = row;
+      cand_key[half] = ((unsigned long long)hmax << 32) | lmax;
+      cand_row[half] = (int)rmin;
     }
   };
   if (cg == 0) candidate(fabs(v[0]), false);
@@ -84,14 +81,10 @@ __device__ inline bool gauss_jordan_sub(double* S, double* X, double* aux) {
 #pragma unroll
     for (int jj = 0; jj < 16; ++jj) {
       const int j = 16 * blk + jj;
-      double best = cand_val[0];
+      const unsigned long long k0 = cand_key[0], k1 = cand_key[1];
       int p = cand_row[0];
-      const double b1 = cand_val[1];
       const int p1 = cand_row[1];
-      if (b1 > best || (b1 == best && p1 < p)) {
-        best = b1;
-        p = p1;
-      }
+      if (k1 > k0 || (k1 == k0 && p1 < p)) p = p1;
       const bool mine = r == p;
       if (mine) {
 #pragma unroll
