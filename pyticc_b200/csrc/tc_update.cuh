@@ -547,7 +547,8 @@ __device__ inline bool tc_update_unit(TcState& s, const TcMaps& maps, int b, int
 // the lower tile (jt, kb) for jt > kb) and P^-1 from the pivot panel at pinv_block0.  Writes
 // the update's A panel (cold) and B panel (U) of column tile jt, U into that lower tile and,
 // for jt = kb + 1, the old rows into `Cb` and U into the rows K (both read by the next
-// pivot's update later in this launch).  Ends with every store complete.
+// pivot's update later in this launch).  Ends with the panels written and the shared buffers
+// free; the store of U's tile may still be in flight (this thread waits for it before exit).
 __device__ inline bool tc_rowpanel_unit(TcState& s, const TcMaps& maps, float* split, int pinv_block0, int b, int kb, int jt, double* Mb, long long ld, double* Cb, int* abort_flag,
                                         int* status) {
   const int tid = threadIdx.x;
@@ -600,12 +601,17 @@ __device__ inline bool tc_rowpanel_unit(TcState& s, const TcMaps& maps, float* s
   fence_proxy_async_shared();
   __syncthreads();
   if (tid == 0) {
-    const uint64_t once = l2_policy_evict_first();
-    for (int q = 0; q < 8; ++q) tma_store_3d(&maps.matrix, s.base_u + (uint32_t)q * kTcCChunkBytes, cx + 16 * q, cy, b, once);
+    // the B panel first, in a bulk group of its own: it must be written before the unit's flag
+    // is released; U's tile is read in this launch by nobody, so its store only has to have
+    // read the C buffer before the buffers are reused
     bulk_copy_s2g(split + (long long)tc_split_block(b, 1, s.nt, jt, 0) * kTcArrayFloats, s.base_u + kTcStageOffset, kTcStages * kTcStageBytes);
     bulk_commit();
-    bulk_wait_all();  // written before the unit's flag is released, and the buffers free
+    const uint64_t once = l2_policy_evict_first();
+    for (int q = 0; q < 8; ++q) tma_store_3d(&maps.matrix, s.base_u + (uint32_t)q * kTcCChunkBytes, cx + 16 * q, cy, b, once);
+    bulk_commit();
+    asm volatile("cp.async.bulk.wait_group 1;" ::: "memory");  // the B panel is written
     fence_proxy_async_global();
+    bulk_wait_read_all();  // and both buffers have been read out
   }
   ++s.tile;
   __syncthreads();
