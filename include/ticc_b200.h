@@ -154,6 +154,18 @@ int ticc_ldmd_propagate_blocks(void* Y, int is_complex, const double* energies, 
                                long long W_end_stride, long long W_block_stride, int n_sector, int n_channel, int n_block, int precision,
                                void* workspace, size_t workspace_bytes, int* device_status, void* stream);
 
+/* Analytic interaction PES on the atom-diatom tensor grid, in device memory (the host
+ * evaluation it replaces: src/pyticc/pes/adiabatic.py:109-137, get_Vgrid_atom_diatom, R x r x
+ * theta in meshgrid "ij" order).  For a PES in the Legendre-expansion form
+ *     V(R, r, theta) = sum_t P_lam[t](cos theta) f_t(R) g_t(r - re),  g_t(d) = sum_q poly[t][q] d^q,
+ *     f_t(R) = sum_p primitive(prim_kind[t][p], params[t][p][0..2], R),
+ * writes V[a][i][k] = V(R[a], r[i], acos(x[k])) (device arrays R, r, x, V; V of n_R * n_r * n_x
+ * doubles).  Primitive kinds: 0 a R^-b, 1 a exp(-b (R - c)), 2 a exp(-((R - c)/b)^2),
+ * 3 a ((b/R)^12 - 2 (b/R)^6).  The term tables are host arrays laid out with 4 primitives
+ * (3 parameters each) and 4 polynomial coefficients per term; at most 16 terms, lam <= 32. */
+int ticc_pes_legendre_grid(const double* R, int n_R, const double* r, int n_r, const double* x, int n_x, int n_terms, const int* lam, const int* n_prim,
+                           const int* prim_kind, const double* prim_params, const int* n_poly, const double* poly, double re, double* V, void* stream);
+
 /* ---- PotentialGrid contraction and W assembly --------------------------------
  * V_K(R) = norm [(B_r v(R)) B_r^T + (B_i v(R)) B_i^T] per K group, scattered into the
  * (n_R, n_channel, n_channel) block-diagonal V.  Replaces contract_device /

@@ -12,6 +12,7 @@ from .cross_section import PartialCrossSections, partial_cross_sections
 from .energy import get_Etot
 from .match import get_Bmat_BF_to_SF, get_Smat, modified_bessel_K_logD, riccati_bessel_jy, transform_logD_BF_to_SF
 from .pes import PESWrapper
+from .pes_analytic import LegendrePES, LegendreTerm, Primitive
 from .propagation import PartialWaveSweep, Propagation, build_radial_sectors, propagate_logD, solve_sweep
 from .kblock import KBlock, build_cs_blocks, build_nncc_blocks
 from .result import CoupledStatesResult, KBlockResult, ScatteringResult, Timing
@@ -20,8 +21,8 @@ from .system import Approx, ChannelSpec, ScatteringType, ScattSystem, build_Scat
 
 __all__ = [
     "AMU2AU", "AU2CM", "AU2K", "CM2AU", "K2AU",
-    "Approx", "AtomSpec", "Channel", "ChannelBasis", "ChannelSpec", "CoupledStatesResult", "DiatomBasis", "DiatomSpec", "KBlock", "KBlockResult",
-    "PESWrapper", "PartialCrossSections", "PartialWaveSweep", "PotentialGrid",
+    "Approx", "AtomSpec", "Channel", "ChannelBasis", "ChannelSpec", "CoupledStatesResult", "DiatomBasis", "DiatomSpec", "KBlock", "KBlockResult", "LegendrePES", "LegendreTerm",
+    "PESWrapper", "Primitive", "PartialCrossSections", "PartialWaveSweep", "PotentialGrid",
     "Propagation", "RovibBasis", "ScattHamiltonian", "ScattSystem", "ScatteringResult", "ScatteringType", "Timing",
     "build_ChannelBasis", "build_RovibDVR", "build_ScattSystem", "build_SineDVR", "build_cs_blocks", "build_k_blocks", "build_nncc_blocks",
     "build_radial_sectors", "finalize_K_block", "get_Bmat_BF_to_SF",

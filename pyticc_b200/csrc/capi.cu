@@ -14,6 +14,7 @@
 #include "learned.cuh"
 #include "ldmd.cuh"
 #include "match.cuh"
+#include "pes.cuh"
 #include "sweep.cuh"
 #include "tc_update.cuh"
 
@@ -292,6 +293,44 @@ int ticc_contract(const double* rows_real, const double* rows_imag, const int* g
   }
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_contract");
+}
+
+// ---- analytic PES on the device -----------------------------------------------------------------
+int ticc_pes_legendre_grid(const double* R, int n_R, const double* r, int n_r, const double* x, int n_x, int n_terms, const int* lam, const int* n_prim,
+                           const int* prim_kind, const double* prim_params, const int* n_poly, const double* poly, double re, double* V, void* stream) {
+  if (R == nullptr || r == nullptr || x == nullptr || V == nullptr || lam == nullptr || n_prim == nullptr || prim_kind == nullptr || prim_params == nullptr ||
+      n_poly == nullptr || poly == nullptr)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_pes_legendre_grid: null pointer");
+  if (n_R < 0 || n_r < 1 || n_x < 1 || n_terms < 1 || n_terms > ticc::kPesMaxTerms)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_pes_legendre_grid: n_R=%d n_r=%d n_x=%d n_terms=%d (at most %d terms)", n_R, n_r, n_x, n_terms, ticc::kPesMaxTerms);
+  ticc::PesTable tab{};
+  tab.n_terms = n_terms;
+  tab.re = re;
+  tab.lmax = 0;
+  for (int t = 0; t < n_terms; ++t) {
+    if (lam[t] < 0 || lam[t] > ticc::kPesMaxLam || n_prim[t] < 0 || n_prim[t] > ticc::kPesMaxPrim || n_poly[t] < 0 || n_poly[t] > ticc::kPesMaxPoly)
+      return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_pes_legendre_grid: term %d has lam=%d, %d primitives, %d polynomial coefficients (at most %d, %d, %d)", t, lam[t],
+                  n_prim[t], n_poly[t], ticc::kPesMaxLam, ticc::kPesMaxPrim, ticc::kPesMaxPoly);
+    tab.lam[t] = lam[t];
+    tab.lmax = lam[t] > tab.lmax ? lam[t] : tab.lmax;
+    tab.n_prim[t] = n_prim[t];
+    tab.n_poly[t] = n_poly[t];
+    for (int p = 0; p < n_prim[t]; ++p) {
+      const int k = prim_kind[t * ticc::kPesMaxPrim + p];
+      if (k < ticc::kPesPower || k > ticc::kPesLJ) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_pes_legendre_grid: term %d primitive %d has unknown kind %d", t, p, k);
+      tab.kind[t][p] = k;
+      tab.a[t][p] = prim_params[(t * ticc::kPesMaxPrim + p) * 3 + 0];
+      tab.b[t][p] = prim_params[(t * ticc::kPesMaxPrim + p) * 3 + 1];
+      tab.c[t][p] = prim_params[(t * ticc::kPesMaxPrim + p) * 3 + 2];
+    }
+    for (int q = 0; q < n_poly[t]; ++q) tab.poly[t][q] = poly[t * ticc::kPesMaxPoly + q];
+  }
+  if (n_R == 0) return TICC_OK;
+  const long long total = (long long)n_R * n_r * n_x;
+  ticc::pes_legendre_kernel<<<ticc::grid_for(total, 256), 256, 0, as_stream(stream)>>>(tab, R, n_R, r, n_r, x, n_x, V);
+  ticc::note_launch();
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_pes_legendre_grid");
 }
 
 // ---- BF -> SF transform ------------------------------------------------------------------------------

@@ -23,6 +23,7 @@ from ..match.asymptotic import get_Bmat_BF_to_SF, transform_device
 from ..match.smatrix import get_Smat_device, open_blocks_to_host
 from ..matrix.interaction import DeviceBasisCache, VBasisBF, contract_device, prepare_atom_diatom, prepare_diatom_diatom
 from ..pes import PESWrapper, get_Vgrid_atom_diatom, get_Vgrid_diatom_diatom
+from ..pes_analytic import LegendrePES
 from ..propagation.config import Propagation
 from ..propagation.grid import RadialSector, build_radial_sectors, radial_points_of
 from ..kblock import KBlock, build_cs_blocks, build_nncc_blocks
@@ -123,8 +124,18 @@ def prepare_potential(system: ScattSystem, boundaries: Sequence[float], half_ste
         parity = system.channel_spec.exchange_parity_Y
         cos_theta, w = gauss_legendre_dvr(-1.0, 1.0, n_theta, symmetry=parity != 0)
         radial = system.monomer_Y.rovib.grids
-        values = get_Vgrid_atom_diatom(system.potential, points, radial, np.arccos(cos_theta))
+        device_values = None
+        if isinstance(system.potential, LegendrePES) and torch.cuda.is_available():
+            # an analytic PES in the Legendre form is evaluated on the device, straight into
+            # the grid the propagation reads (pes_analytic.py, ticc_pes_legendre_grid)
+            device = torch.device("cuda", torch.cuda.current_device())
+            device_values = system.potential.grid_device(points, radial, cos_theta, device)
+            values = device_values.cpu().numpy().reshape(points.size, radial.size, cos_theta.size)
+        else:
+            values = get_Vgrid_atom_diatom(system.potential, points, radial, np.arccos(cos_theta))
         grid = PotentialGrid(b, h, sectors, points, system.scattering_type, (("r", radial), ("cos_theta", cos_theta)), (("theta", w),), values)
+        if device_values is not None:
+            grid._device_cache[(device.type, device.index)] = device_values
     else:
         cX, wX = gauss_legendre_dvr(-1.0, 1.0, int(quadrature.get("n_theta_X", 15)))
         cY, wY = gauss_legendre_dvr(-1.0, 1.0, int(quadrature.get("n_theta_Y", 15)))
