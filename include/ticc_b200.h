@@ -154,6 +154,17 @@ int ticc_ldmd_propagate_blocks(void* Y, int is_complex, const double* energies, 
                                long long W_end_stride, long long W_block_stride, int n_sector, int n_channel, int n_block, int precision,
                                void* workspace, size_t workspace_bytes, int* device_status, void* stream);
 
+/* One block of a state-resolved (diabatic) atom-diatom contraction, the weighted products of
+ * src/pyticc/matrix/interaction/diabatic_atom_diatom.py:262-287 (_contract_weighted_basis):
+ *     X(R)[i][j] = sum_q A[i][q] weights[R * w_stride + q] B[j][q]
+ * written to out[R][pos_a[i]][pos_b[j]] (out: n_R x n x n, device) and, with `mirror`, also to
+ * out[R][pos_b[j]][pos_a[i]] (the coupling blocks of two electronic states).  A `symmetric`
+ * block (B == A, pos_b == pos_a: a diagonal block) is computed on its lower half and mirrored,
+ * so it is exactly symmetric.  Entries outside the block are left as they are (the caller
+ * zeroes out).  All arrays are device arrays; A and B have row stride n_grid. */
+int ticc_contract_block(const double* A, int n_a, const double* B, int n_b, int n_grid, const double* weights, long long w_stride, int n_R, const int* pos_a,
+                        const int* pos_b, int symmetric, int mirror, int n, double* out, void* stream);
+
 /* Analytic interaction PES on the atom-diatom tensor grid, in device memory (the host
  * evaluation it replaces: src/pyticc/pes/adiabatic.py:109-137, get_Vgrid_atom_diatom, R x r x
  * theta in meshgrid "ij" order).  For a PES in the Legendre-expansion form

@@ -295,6 +295,22 @@ int ticc_contract(const double* rows_real, const double* rows_imag, const int* g
   return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_contract");
 }
 
+// ---- one block of a state-resolved contraction ----------------------------------------------------
+int ticc_contract_block(const double* A, int n_a, const double* B, int n_b, int n_grid, const double* weights, long long w_stride, int n_R, const int* pos_a,
+                        const int* pos_b, int symmetric, int mirror, int n, double* out, void* stream) {
+  if (A == nullptr || B == nullptr || weights == nullptr || pos_a == nullptr || pos_b == nullptr || out == nullptr)
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_contract_block: null pointer");
+  if (n_a < 0 || n_b < 0 || n_grid < 1 || n_R < 0 || n < 1 || w_stride < n_grid || (symmetric && (n_a != n_b || A != B || pos_a != pos_b)))
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_contract_block: n_a=%d n_b=%d n_grid=%d n_R=%d n=%d w_stride=%lld symmetric=%d (a symmetric block has B = A)", n_a, n_b,
+                n_grid, n_R, n, w_stride, symmetric);
+  if (n_a == 0 || n_b == 0 || n_R == 0) return TICC_OK;
+  const dim3 grid((n_a + ticc::kCTile - 1) / ticc::kCTile, (n_b + ticc::kCTile - 1) / ticc::kCTile, n_R);
+  ticc::weighted_block_kernel<<<grid, 256, 0, as_stream(stream)>>>(A, n_a, B, n_b, n_grid, weights, w_stride, pos_a, pos_b, symmetric, mirror, n, out);
+  ticc::note_launch();
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_contract_block");
+}
+
 // ---- analytic PES on the device -----------------------------------------------------------------
 int ticc_pes_legendre_grid(const double* R, int n_R, const double* r, int n_r, const double* x, int n_x, int n_terms, const int* lam, const int* n_prim,
                            const int* prim_kind, const double* prim_params, const int* n_poly, const double* poly, double re, double* V, void* stream) {

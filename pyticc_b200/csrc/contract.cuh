@@ -94,4 +94,54 @@ __global__ void __launch_bounds__(256) contract_group_kernel(const double* __res
     }
 }
 
+// One block of a state-resolved (diabatic) contraction at every R:
+//     X(R)[i][j] = sum_q A[i][q] w(R)[q] B[j][q],   A: n_a x n_grid, B: n_b x n_grid (row strides n_grid)
+// written to out(R)[pos_a[i]][pos_b[j]] and, with `mirror`, also to out(R)[pos_b[j]][pos_a[i]].
+// A symmetric block (`symmetric`: B is A and pos_b is pos_a) computes only i >= j and writes
+// both (i, j) and (j, i), so the block is exactly symmetric.  grid: (tiles of A, tiles of B,
+// n_R); block 16 x 16 threads, 2 x 2 outputs each.
+__global__ void __launch_bounds__(256) weighted_block_kernel(const double* __restrict__ A, int n_a, const double* __restrict__ B, int n_b, int n_grid, const double* __restrict__ w,
+                                                             long long w_stride, const int* __restrict__ pos_a, const int* __restrict__ pos_b, int symmetric, int mirror, int n,
+                                                             double* __restrict__ out) {
+  const int ti = blockIdx.x, tj = blockIdx.y, R = blockIdx.z;
+  if (symmetric && tj > ti) return;
+  __shared__ double As[kCTile][kCTile + 1];
+  __shared__ double Bs[kCTile][kCTile + 1];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int i0 = ti * kCTile, j0 = tj * kCTile;
+  const double* wr = w + (long long)R * w_stride;
+  double acc[2][2] = {};
+  for (int q0 = 0; q0 < n_grid; q0 += kCTile) {
+    for (int e = threadIdx.x; e < kCTile * kCTile; e += 256) {
+      const int rr = e / kCTile, qq = e % kCTile, q = q0 + qq;
+      const bool inq = q < n_grid;
+      As[rr][qq] = (inq && i0 + rr < n_a) ? A[(long long)(i0 + rr) * n_grid + q] * wr[q] : 0.0;
+      Bs[rr][qq] = (inq && j0 + rr < n_b) ? B[(long long)(j0 + rr) * n_grid + q] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int qq = 0; qq < kCTile; ++qq) {
+      const double a0 = As[ty][qq], a1 = As[ty + 16][qq];
+      const double b0 = Bs[tx][qq], b1 = Bs[tx + 16][qq];
+      acc[0][0] = fma(a0, b0, acc[0][0]);
+      acc[0][1] = fma(a0, b1, acc[0][1]);
+      acc[1][0] = fma(a1, b0, acc[1][0]);
+      acc[1][1] = fma(a1, b1, acc[1][1]);
+    }
+    __syncthreads();
+  }
+  double* o = out + (long long)R * n * n;
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const int i = i0 + ty + 16 * u, j = j0 + tx + 16 * v;
+      if (i >= n_a || j >= n_b || (symmetric && j > i)) continue;
+      const int pa = pos_a[i], pb = pos_b[j];
+      o[(long long)pa * n + pb] = acc[u][v];
+      if (mirror || (symmetric && i != j)) o[(long long)pb * n + pa] = acc[u][v];
+    }
+}
+
+
 }  // namespace ticc

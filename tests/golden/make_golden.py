@@ -686,6 +686,44 @@ def make_dropin() -> None:
     )
 
 
+def make_contract_families() -> None:
+    """Electric-field SF and diabatic contractions: the reference's host functions on seeded
+    synthetic bases (atom_diatom.py:208-267, diabatic_atom_diatom.py:325-440)."""
+    from pyticc.matrix.interaction import atom_diatom as ref_ad
+    from pyticc.matrix.interaction import diabatic_atom_diatom as ref_dia
+
+    rng = np.random.default_rng(404)
+    grid_shape = (3, 4, 5, 2)
+    n_grid, n_channel = int(np.prod(grid_shape)), 11
+    B_cos, B_sin = rng.normal(size=(n_channel, n_grid)), rng.normal(size=(n_channel, n_grid))
+    sf = ref_ad.AtomDiatomVBasisElectricSF(n_channel=n_channel, grid_shape=grid_shape, r=np.zeros(3), gamma=np.zeros((4, 5, 2)), B_cos=B_cos, B_sin=B_sin)
+    sf_pot = rng.normal(size=(3, *grid_shape))
+    sf_V = ref_ad.contract_electric_sf(sf, sf_pot)
+    sf_V_subset = ref_ad.contract_electric_sf(sf, sf_pot[1], (9, 2, 4, 0))
+
+    n_theta, grids = 6, (np.linspace(1.0, 2.0, 4), np.linspace(1.2, 2.4, 5))
+    coupling_grid = np.linspace(1.0, 2.4, 7)
+    groups = {(0, 0): (0, 3, 5), (0, 1): (1, 6), (1, 0): (2, 7, 8, 9), (1, 1): (4, 10, 11)}
+    n_dia = 12
+    B_diag = {k: rng.normal(size=(len(v), grids[k[0]].size * n_theta)) for k, v in groups.items()}
+    B_coup = {k: rng.normal(size=(len(v), coupling_grid.size * n_theta)) for k, v in groups.items()}
+    dia = ref_dia.DiabaticVBasisBF(n_channel=n_dia, n_state=2, theta=np.linspace(0.1, 3.0, n_theta), diagonal_grids=grids, coupling_grid=coupling_grid,
+                                   channel_indices=groups, B_diagonal=B_diag, B_coupling=B_coup)
+    d0, d1 = rng.normal(size=(3, grids[0].size, n_theta)), rng.normal(size=(3, grids[1].size, n_theta))
+    c = rng.normal(size=(3, coupling_grid.size, n_theta, 2, 2))
+    c = 0.5 * (c + np.swapaxes(c, -2, -1))
+    dia_V = ref_dia.contract(dia, ref_dia.DiabaticVGridBF(diagonal=(d0, d1), coupling=c))
+    dia_V_subset = ref_dia.contract(dia, ref_dia.DiabaticVGridBF(diagonal=(d0[2], d1[2]), coupling=c[2]), (11, 3, 7, 0, 10, 2))
+    _save(
+        "contract_families",
+        {"grid_shape": list(grid_shape), "groups": {f"{k[0]},{k[1]}": list(v) for k, v in groups.items()}, "n_theta": n_theta, "sf_subset": [9, 2, 4, 0],
+         "dia_subset": [11, 3, 7, 0, 10, 2]},
+        sf_B_cos=B_cos, sf_B_sin=B_sin, sf_pot=sf_pot, sf_V=sf_V, sf_V_subset=sf_V_subset,
+        dia_grid0=grids[0], dia_grid1=grids[1], dia_coupling_grid=coupling_grid, dia_d0=d0, dia_d1=d1, dia_c=c, dia_V=dia_V, dia_V_subset=dia_V_subset,
+        **{f"dia_Bd_{k[0]}_{k[1]}": v for k, v in B_diag.items()}, **{f"dia_Bc_{k[0]}_{k[1]}": v for k, v in B_coup.items()},
+    )
+
+
 MAKERS = {
     "ldmd": make_ldmd,
     "contract": make_contract,
@@ -699,6 +737,7 @@ MAKERS = {
     "kblocks": make_kblocks,
     "solve_kblocks": make_solve_kblocks,
     "dropin": make_dropin,
+    "contract_families": make_contract_families,
 }
 # benchmark-size fixtures: run by name only (tens of minutes of CPU in total);
 # ``full_morse`` takes optional parities after its name: ``make_golden.py <src> full_morse -1``
