@@ -165,6 +165,16 @@ int ticc_ldmd_propagate_blocks(void* Y, int is_complex, const double* energies, 
 int ticc_contract_block(const double* A, int n_a, const double* B, int n_b, int n_grid, const double* weights, long long w_stride, int n_R, const int* pos_a,
                         const int* pos_b, int symmetric, int mirror, int n, double* out, void* stream);
 
+/* Packed lower-triangle channel pairs of the fine-structure contractions into matrices (the
+ * scatter of src/pyticc/matrix/interaction/fs_diatom_diatom.py:383-391 and
+ * fs_diatom_diatom_spin.py:463-482): for pair p = (pair_rows[p], pair_cols[p]) (rows >= cols)
+ * and every R, the value src[R * src_stride + p] (real) or the complex double at element p
+ * (is_complex; conjugated where reversed[p] is non-zero) goes to out[R][i][j] and, mirrored
+ * (conjugated when complex), to out[R][j][i]; a complex diagonal element keeps its real part.
+ * out: n_R x n x n doubles or interleaved complex doubles.  Device arrays; reversed may be null. */
+int ticc_pairs_to_matrix(const double* src, int is_complex, long long src_stride, int n_pairs, const int* pair_rows, const int* pair_cols,
+                         const unsigned char* reversed, int n, int n_R, double* out, void* stream);
+
 /* Analytic interaction PES on the atom-diatom tensor grid, in device memory (the host
  * evaluation it replaces: src/pyticc/pes/adiabatic.py:109-137, get_Vgrid_atom_diatom, R x r x
  * theta in meshgrid "ij" order).  For a PES in the Legendre-expansion form

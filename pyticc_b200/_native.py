@@ -58,6 +58,7 @@ SIGNATURES: dict[str, tuple[list, type]] = {
     "ticc_ldmd_propagate_blocks": ([_P, _I, _P, _I, _D, _P, _P, _LL, _P, _LL, _P, _LL, _LL, _I, _I, _I, _I, _P, _SZ, _P, _P], _I),
     "ticc_contract": ([_P, _P, ctypes.POINTER(_I), _I, _P, _I, _D, _P, _LL, _I, _I, _P, _P, _P, _D, _P, _P], _I),
     "ticc_contract_block": ([_P, _I, _P, _I, _I, _P, _LL, _I, _P, _P, _I, _I, _I, _P, _P], _I),
+    "ticc_pairs_to_matrix": ([_P, _I, _LL, _I, _P, _P, _P, _I, _I, _P, _P], _I),
     "ticc_pes_legendre_grid": ([_P, _I, _P, _I, _P, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_D), ctypes.POINTER(_I), ctypes.POINTER(_D), _D, _P, _P], _I),
     "ticc_transform_workspace_size": ([_I, _I, _I, _PSZ], _I),
     "ticc_transform_bf_to_sf": ([_P, _P, _P, _I, _I, _I, _P, _SZ, _P], _I),

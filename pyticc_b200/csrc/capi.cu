@@ -311,6 +311,20 @@ int ticc_contract_block(const double* A, int n_a, const double* B, int n_b, int 
   return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_contract_block");
 }
 
+// ---- packed channel pairs into matrices (fine-structure families) --------------------------------
+int ticc_pairs_to_matrix(const double* src, int is_complex, long long src_stride, int n_pairs, const int* pair_rows, const int* pair_cols,
+                         const unsigned char* reversed, int n, int n_R, double* out, void* stream) {
+  if (src == nullptr || pair_rows == nullptr || pair_cols == nullptr || out == nullptr) return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_pairs_to_matrix: null pointer");
+  if (n_pairs < 0 || n < 1 || n_R < 0 || src_stride < (long long)n_pairs * (is_complex ? 2 : 1))
+    return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_pairs_to_matrix: n_pairs=%d n=%d n_R=%d src_stride=%lld", n_pairs, n, n_R, src_stride);
+  if (n_pairs == 0 || n_R == 0) return TICC_OK;
+  ticc::pairs_to_matrix_kernel<<<ticc::grid_for((long long)n_R * n_pairs, 256), 256, 0, as_stream(stream)>>>(src, is_complex, src_stride, n_pairs, pair_rows, pair_cols, reversed, n,
+                                                                                                          n_R, out);
+  ticc::note_launch();
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_pairs_to_matrix");
+}
+
 // ---- analytic PES on the device -----------------------------------------------------------------
 int ticc_pes_legendre_grid(const double* R, int n_R, const double* r, int n_r, const double* x, int n_x, int n_terms, const int* lam, const int* n_prim,
                            const int* prim_kind, const double* prim_params, const int* n_poly, const double* poly, double re, double* V, void* stream) {

@@ -144,4 +144,40 @@ __global__ void __launch_bounds__(256) weighted_block_kernel(const double* __res
 }
 
 
+// Packed lower-triangle channel pairs of a fine-structure contraction into matrices: for every R
+// and pair p = (i, j) = (pair_rows[p], pair_cols[p]), i >= j, with value v = src(R, p):
+//   real (scalar FS):   out[i][j] = out[j][i] = v;
+//   complex (spin FS):  v is conjugated where reversed[p]; out[i][j] = v, out[j][i] = conj(v),
+//                       a diagonal element keeps the real part.
+// src: n_R rows of src_stride elements (doubles, or interleaved complex doubles); out: n_R x n x n.
+__global__ void __launch_bounds__(256) pairs_to_matrix_kernel(const double* __restrict__ src, int is_complex, long long src_stride, int n_pairs, const int* __restrict__ pair_rows,
+                                                              const int* __restrict__ pair_cols, const unsigned char* __restrict__ reversed, int n, int n_R,
+                                                              double* __restrict__ out) {
+  const long long total = (long long)n_R * n_pairs;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int R = (int)(e / n_pairs), p = (int)(e % n_pairs);
+    const int i = pair_rows[p], j = pair_cols[p];
+    if (is_complex) {
+      const double re = src[(long long)R * src_stride + 2 * p];
+      double im = src[(long long)R * src_stride + 2 * p + 1];
+      if (reversed != nullptr && reversed[p]) im = -im;
+      double* o = out + 2 * (long long)R * n * n;
+      if (i == j) {
+        o[2 * ((long long)i * n + i)] = re;
+        o[2 * ((long long)i * n + i) + 1] = 0.0;
+      } else {
+        o[2 * ((long long)i * n + j)] = re;
+        o[2 * ((long long)i * n + j) + 1] = im;
+        o[2 * ((long long)j * n + i)] = re;
+        o[2 * ((long long)j * n + i) + 1] = -im;
+      }
+    } else {
+      const double v = src[(long long)R * src_stride + p];
+      double* o = out + (long long)R * n * n;
+      o[(long long)i * n + j] = v;
+      o[(long long)j * n + i] = v;
+    }
+  }
+}
+
 }  // namespace ticc

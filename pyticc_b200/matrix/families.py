@@ -1,6 +1,7 @@
-"""Further contraction families on the GPU: electric-field space-fixed and diabatic atom-diatom.
+"""Further contraction families on the GPU: electric-field space-fixed and diabatic atom-diatom,
+and the fine-structure diatom-diatom families (scalar and spin-resolved).
 
-Both are the weighted-row contraction of the exact-CC path with another axis:
+The first two are the weighted-row contraction of the exact-CC path with another axis:
 
 * electric-field SF (reference ``src/pyticc/matrix/interaction/atom_diatom.py:26-80, 271-345``):
   ``V = sym(B_cos diag(v) B_cos^T + B_sin diag(v) B_sin^T)``, one group of rows, so it runs on
@@ -10,9 +11,13 @@ Both are the weighted-row contraction of the exact-CC path with another axis:
   a coupling block ``B_a diag(v_ab) B_b^T`` placed at (a, b) and mirrored to (b, a); every block
   is one ``ticc_contract_block`` launch into a zeroed output.
 
+The fine-structure families contract with a packed kernel over lower-triangle channel pairs
+(a cuBLAS GEMM) and scatter the pairs into symmetric or Hermitian matrices (``ticc_pairs_to_matrix``).
+
 The functions take the reference's basis objects as they are (attributes are read by name), so
-they are drop-ins for the reference's ``contract_electric_sf_device`` and the diabatic
-``contract_device``; the dataclasses below mirror the reference's for callers without it.
+they are drop-ins for the reference's ``contract_electric_sf_device``, the diabatic and the
+fine-structure ``contract_device``; the dataclasses below mirror the reference's for callers
+without it.
 """
 
 from __future__ import annotations
@@ -217,3 +222,118 @@ def contract_diabatic_device(V_basis, basis_device, potential, device, channel_i
                     Bb = basis_device.B_coupling[(b, K)].index_select(0, rows_b).contiguous()
                     launch(A, Bb, coupling_flat[:, :, a, b].contiguous(), pos_a, pos_b, False, True)
     return out if flags[0] else out[0]
+
+
+# ---- fine-structure diatom-diatom (scalar and spin-resolved) -----------------------------------------
+# Both contract the PES grid with a packed kernel over lower-triangle channel pairs,
+#   contracted(R, p) = sum_k potential(R, k) kernel(k, packed(p)),
+# a plain GEMM (cuBLAS through torch), then scatter the pairs into matrices (ticc_pairs_to_matrix):
+# symmetric for the scalar family (fs_diatom_diatom.py:356-470), Hermitian with conjugation of
+# reversed pairs for the spin-resolved one (fs_diatom_diatom_spin.py:459-550).
+_KERNEL_CHUNK_BYTES = 256 * 1024**2
+
+
+def packed_positions(n_channel: int, indices: tuple[int, ...]):
+    """Selected lower-triangle pairs and their positions in the complete packed order
+    (the reference's packing, fs_diatom_diatom.py:336-349)."""
+    indices = _selection(n_channel, indices)
+    pair_rows, pair_columns = np.tril_indices(len(indices))
+    selected = np.asarray(indices, dtype=np.int64)
+    rows, cols = selected[pair_rows], selected[pair_columns]
+    hi, lo = np.maximum(rows, cols), np.minimum(rows, cols)
+    return pair_rows.astype(np.int64), pair_columns.astype(np.int64), (hi * (hi + 1) // 2 + lo).astype(np.int64), selected
+
+
+@dataclass(frozen=True)
+class FSKernelDevice:
+    """The packed kernel (n_k, n_packed) on the device, or None to stream it from the host."""
+
+    kernel: NDArray
+    resident: torch.Tensor | None
+
+
+def device_basis_fs(V_basis, device) -> FSKernelDevice:
+    """Keep kernels up to 256 MiB resident on the device; stream larger ones by pair chunks."""
+    dev = nat.require_cuda(device)
+    k = np.asarray(V_basis.kernel)
+    return FSKernelDevice(k, torch.as_tensor(k.reshape(-1, k.shape[-1]), device=dev) if k.nbytes <= _KERNEL_CHUNK_BYTES else None)
+
+
+def _contract_packed(batches: torch.Tensor, basis_device: FSKernelDevice, n_channel: int, channel_indices, hermitian: bool, dev) -> torch.Tensor:
+    indices = tuple(range(n_channel)) if channel_indices is None else tuple(channel_indices)
+    pair_rows, pair_cols, packed, selected = packed_positions(n_channel, indices)
+    host_kernel = basis_device.kernel.reshape(-1, basis_device.kernel.shape[-1])
+    dtype = torch.complex128 if (hermitian and (torch.is_complex(batches) or np.iscomplexobj(host_kernel))) else torch.float64
+    lhs = batches.to(dev, dtype)
+    n_k = lhs.shape[1]
+    itemsize = 16 if dtype == torch.complex128 else 8
+    per_chunk = max(1, _KERNEL_CHUNK_BYTES // (n_k * itemsize))
+    contracted = torch.empty((lhs.shape[0], packed.size), dtype=dtype, device=dev)
+    for start in range(0, packed.size, per_chunk):
+        chunk = packed[start : start + per_chunk]
+        if basis_device.resident is not None:
+            kern = basis_device.resident.index_select(1, torch.as_tensor(chunk, device=dev)).to(dtype)
+        else:
+            kern = torch.as_tensor(np.ascontiguousarray(host_kernel[:, chunk]), device=dev).to(dtype)
+        contracted[:, start : start + chunk.size] = lhs @ kern
+    n = len(indices)
+    is_complex = dtype == torch.complex128
+    out = torch.zeros((lhs.shape[0], n, n), dtype=dtype, device=dev)
+    src = torch.view_as_real(contracted).reshape(lhs.shape[0], -1) if is_complex else contracted
+    reversed_pairs = None
+    if is_complex:
+        reversed_pairs = torch.as_tensor((selected[pair_rows] < selected[pair_cols]).astype(np.uint8), device=dev)
+    pr = torch.as_tensor(pair_rows.astype(np.int32), device=dev)
+    pc = torch.as_tensor(pair_cols.astype(np.int32), device=dev)
+    lib = nat.load_library()
+    with torch.cuda.device(dev):
+        nat.check(
+            lib.ticc_pairs_to_matrix(nat.ptr(src), int(is_complex), src.stride(0), int(packed.size), nat.ptr(pr), nat.ptr(pc), nat.ptr(reversed_pairs), n, lhs.shape[0],
+                                     nat.ptr(torch.view_as_real(out) if is_complex else out), nat.stream_handle(dev)),
+            "ticc_pairs_to_matrix",
+        )
+    return out
+
+
+def contract_fs_device(V_basis, basis_device, potential, device, channel_indices: Sequence[int] | None = None) -> torch.Tensor:
+    """Scalar PES into two-fine-structure-diatom channel matrices (fs_diatom_diatom.py:417-470)."""
+    dev = nat.require_cuda(device)
+    grid_shape = tuple(V_basis.grid_shape)
+    n_grid = prod(grid_shape)
+    values = potential if isinstance(potential, torch.Tensor) else torch.as_tensor(np.asarray(potential, dtype=np.float64))
+    shape = tuple(values.shape)
+    if shape == grid_shape:
+        batches, batched = values.reshape(1, n_grid), False
+    elif len(shape) == len(grid_shape) + 1 and shape[1:] == grid_shape:
+        batches, batched = values.reshape(shape[0], n_grid), True
+    elif len(shape) == 2 and shape[1] == n_grid:
+        batches, batched = values, True
+    else:
+        raise _error(f"Scalar FS diatom-diatom PES grid has shape {shape}, expected {grid_shape} with optional leading R axis")
+    if basis_device is None:
+        basis_device = device_basis_fs(V_basis, dev)
+    V = _contract_packed(batches, basis_device, V_basis.n_channel, channel_indices, False, dev)
+    return V if batched else V[0]
+
+
+def contract_fs_spin_device(V_basis, basis_device, potential, device, channel_indices: Sequence[int] | None = None) -> torch.Tensor:
+    """Spin-resolved orbital PES grids into Hermitian channel matrices (fs_diatom_diatom_spin.py:504-550)."""
+    dev = nat.require_cuda(device)
+    grid_shape = tuple(V_basis.grid_shape)
+    electronic = (len(V_basis.two_total_spins), len(V_basis.orbital_states), len(V_basis.orbital_states))
+    n_grid, n_el = prod(grid_shape), prod(electronic)
+    values = potential if isinstance(potential, torch.Tensor) else torch.as_tensor(np.asarray(potential))
+    shape = tuple(values.shape)
+    expected = (*grid_shape, *electronic)
+    if shape == expected:
+        batches, batched = values.reshape(1, n_grid * n_el), False
+    elif len(shape) == len(expected) + 1 and shape[1:] == expected:
+        batches, batched = values.reshape(shape[0], n_grid * n_el), True
+    elif len(shape) == 3 and shape[1:] == (n_grid, n_el):
+        batches, batched = values.reshape(shape[0], n_grid * n_el), True
+    else:
+        raise _error(f"Spin-resolved FS diatom-diatom PES grid has shape {shape}, expected {expected} with optional leading R axis")
+    if basis_device is None:
+        basis_device = device_basis_fs(V_basis, dev)
+    V = _contract_packed(batches, basis_device, V_basis.n_channel, channel_indices, True, dev)
+    return V if batched else V[0]

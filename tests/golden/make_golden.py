@@ -724,6 +724,36 @@ def make_contract_families() -> None:
     )
 
 
+
+def make_contract_fs() -> None:
+    """Fine-structure diatom-diatom contractions, scalar and spin-resolved: the reference's host
+    functions on seeded synthetic packed kernels (fs_diatom_diatom.py:356-391,
+    fs_diatom_diatom_spin.py:459-482)."""
+    from pyticc.matrix.interaction import fs_diatom_diatom as ref_fs
+    from pyticc.matrix.interaction import fs_diatom_diatom_spin as ref_spin
+    from pyticc.pes.spin_resolved_diatom_diatom import OrbitalState
+
+    rng = np.random.default_rng(505)
+    grid_shape = (2, 2, 3, 2, 2)
+    n_grid, n_channel = int(np.prod(grid_shape)), 7
+    n_packed = n_channel * (n_channel + 1) // 2
+    pr, pc = np.tril_indices(n_channel)
+    kernel = rng.normal(size=(n_grid, n_packed))
+    fs = ref_fs.FSDiatomDiatomVBasis(n_channel=n_channel, grid_shape=grid_shape, pair_rows=pr, pair_columns=pc, kernel=kernel)
+    fs_pot = rng.normal(size=(3, *grid_shape))
+    fs_V = ref_fs.contract(fs, fs_pot)
+    fs_V_subset = ref_fs.contract(fs, fs_pot[0], (5, 1, 6, 2))
+    spins, orbitals = (0, 2), (OrbitalState(0, 0), OrbitalState(2, -2))
+    n_el = len(spins) * len(orbitals) ** 2
+    skernel = rng.normal(size=(n_grid, n_el, n_packed)) + 1j * rng.normal(size=(n_grid, n_el, n_packed))
+    spin = ref_spin.SpinResolvedFSDiatomDiatomVBasis(n_channel=n_channel, grid_shape=grid_shape, two_total_spins=spins, orbital_states=orbitals, pair_rows=pr,
+                                                     pair_columns=pc, kernel=skernel)
+    spin_pot = rng.normal(size=(3, *grid_shape, 2, 2, 2)) + 1j * rng.normal(size=(3, *grid_shape, 2, 2, 2))
+    spin_V = ref_spin.contract(spin, spin_pot)
+    spin_V_subset = ref_spin.contract(spin, spin_pot[1], (6, 0, 3, 4))
+    _save("contract_fs", {"grid_shape": list(grid_shape), "n_channel": n_channel, "fs_subset": [5, 1, 6, 2], "spin_subset": [6, 0, 3, 4], "two_total_spins": list(spins)},
+          fs_kernel=kernel, fs_pot=fs_pot, fs_V=fs_V, fs_V_subset=fs_V_subset, spin_kernel=skernel, spin_pot=spin_pot, spin_V=spin_V, spin_V_subset=spin_V_subset)
+
 MAKERS = {
     "ldmd": make_ldmd,
     "contract": make_contract,
@@ -738,6 +768,7 @@ MAKERS = {
     "solve_kblocks": make_solve_kblocks,
     "dropin": make_dropin,
     "contract_families": make_contract_families,
+    "contract_fs": make_contract_fs,
 }
 # benchmark-size fixtures: run by name only (tens of minutes of CPU in total);
 # ``full_morse`` takes optional parities after its name: ``make_golden.py <src> full_morse -1``

@@ -42,3 +42,41 @@ def test_diabatic_is_blocks_of_state_weighted_products():
             V[np.ix_(ia, ib)] = X
             V[np.ix_(ib, ia)] = X.T
         np.testing.assert_allclose(DATA["dia_V"][R], V, rtol=0, atol=1e-12 * np.abs(V).max())
+
+
+FS = np.load(Path(__file__).parent / "golden" / "contract_fs.npz")
+FS_PARAMS = json.loads(str(FS["params_json"]))
+
+
+def _packed(n_channel, indices):
+    pr, pc = np.tril_indices(len(indices))
+    sel = np.asarray(indices)
+    hi, lo = np.maximum(sel[pr], sel[pc]), np.minimum(sel[pr], sel[pc])
+    return pr, pc, hi * (hi + 1) // 2 + lo, sel
+
+
+def test_scalar_fs_is_a_packed_pair_product_scattered_symmetrically():
+    n, idx = FS_PARAMS["n_channel"], FS_PARAMS["fs_subset"]
+    for pot, want, indices in ((FS["fs_pot"].reshape(3, -1), FS["fs_V"], list(range(n))), (FS["fs_pot"][0].reshape(1, -1), FS["fs_V_subset"][None], idx)):
+        pr, pc, packed, _ = _packed(n, indices)
+        c = pot @ FS["fs_kernel"][:, packed]
+        M = np.zeros((pot.shape[0], len(indices), len(indices)))
+        M[:, pr, pc] = c
+        M[:, pc, pr] = c
+        np.testing.assert_allclose(want, M, rtol=0, atol=1e-12 * np.abs(M).max())
+
+
+def test_spin_fs_is_a_packed_pair_product_scattered_hermitian():
+    n, idx = FS_PARAMS["n_channel"], FS_PARAMS["spin_subset"]
+    k = FS["spin_kernel"].reshape(-1, FS["spin_kernel"].shape[-1])
+    for pot, want, indices in ((FS["spin_pot"].reshape(3, -1), FS["spin_V"], list(range(n))), (FS["spin_pot"][1].reshape(1, -1), FS["spin_V_subset"][None], idx)):
+        pr, pc, packed, sel = _packed(n, indices)
+        c = pot @ k[:, packed]
+        rev = sel[pr] < sel[pc]
+        c[:, rev] = np.conj(c[:, rev])
+        M = np.zeros((pot.shape[0], len(indices), len(indices)), dtype=complex)
+        M[:, pr, pc] = c
+        off = pr != pc
+        M[:, pc[off], pr[off]] = np.conj(c[:, off])
+        M[:, pr[~off], pc[~off]] = np.real(c[:, ~off])
+        np.testing.assert_allclose(want, M, rtol=0, atol=1e-12 * np.abs(M).max())

@@ -64,3 +64,33 @@ def test_diabatic_contraction_matches_reference():
     bad[..., 0, 1] += 1.0
     with pytest.raises(ValueError, match="symmetric"):
         fam.contract_diabatic_device(basis, basis_device, fam.DiabaticVGridBF(diagonal=(DATA["dia_d0"], DATA["dia_d1"]), coupling=bad), dev)
+
+
+FS = np.load(Path(__file__).parent / "golden" / "contract_fs.npz")
+FS_PARAMS = json.loads(str(FS["params_json"]))
+
+
+class _FSBasis:
+    def __init__(self, kernel, spin=False):
+        n = FS_PARAMS["n_channel"]
+        self.n_channel, self.grid_shape, self.kernel = n, tuple(FS_PARAMS["grid_shape"]), kernel
+        self.pair_rows, self.pair_columns = np.tril_indices(n)
+        if spin:
+            self.two_total_spins, self.orbital_states = tuple(FS_PARAMS["two_total_spins"]), (None, None)
+
+
+def test_scalar_fs_contraction_matches_reference():
+    dev = torch.device("cuda", 0)
+    basis = _FSBasis(FS["fs_kernel"])
+    _close(fam.contract_fs_device(basis, fam.device_basis_fs(basis, dev), FS["fs_pot"], dev), FS["fs_V"])
+    _close(fam.contract_fs_device(basis, None, FS["fs_pot"][0], dev, FS_PARAMS["fs_subset"]), FS["fs_V_subset"])
+
+
+def test_spin_fs_contraction_matches_reference_and_is_hermitian():
+    dev = torch.device("cuda", 0)
+    basis = _FSBasis(FS["spin_kernel"], spin=True)
+    V = fam.contract_fs_spin_device(basis, fam.device_basis_fs(basis, dev), FS["spin_pot"], dev)
+    _close(V, FS["spin_V"])
+    Vc = V.cpu().numpy()
+    np.testing.assert_array_equal(Vc, np.conj(np.swapaxes(Vc, -2, -1)))
+    _close(fam.contract_fs_spin_device(basis, None, FS["spin_pot"][1], dev, FS_PARAMS["spin_subset"]), FS["spin_V_subset"])
