@@ -754,6 +754,64 @@ def make_contract_fs() -> None:
     _save("contract_fs", {"grid_shape": list(grid_shape), "n_channel": n_channel, "fs_subset": [5, 1, 6, 2], "spin_subset": [6, 0, 3, 4], "two_total_spins": list(spins)},
           fs_kernel=kernel, fs_pot=fs_pot, fs_V=fs_V, fs_V_subset=fs_V_subset, spin_kernel=skernel, spin_pot=spin_pot, spin_V=spin_V, spin_V_subset=spin_V_subset)
 
+
+def make_delves() -> None:
+    """Delves propagation (propagation/delves.py:54-286) driven by a seeded synthetic surface
+    provider: surfaces whose energies and coefficients vary smoothly with rho and whose count
+    drops from 5 to 4 halfway (a rectangular overlap); inelastic and capture starts."""
+    from pyticc.propagation.delves import propagate_delves as ref_propagate_delves
+    from pyticc.scattering.reactive.delves import DelvesHamiltonian, DelvesSurface
+
+    n_primitive = 6
+
+    class _Basis:
+        rho_min = 2.0
+        mass = (1.0 * AMU, 2.0 * AMU, 19.0 * AMU)
+
+    _Basis.n_primitive = n_primitive
+
+    def surface_at(rho):
+        n = 5 if rho < 4.0 else 4
+        e = np.array([0.02 + 0.01 * k + 0.05 * np.exp(-(rho - 2.0)) * (k + 1) for k in range(n)])
+        th, ph = 0.3 * np.sin(rho), 0.2 * np.cos(0.7 * rho)
+        G = np.eye(n_primitive)
+        for (a, b, ang) in ((0, 1, th), (2, 3, ph), (1, 4, 0.5 * th)):
+            R = np.eye(n_primitive)
+            R[a, a] = R[b, b] = np.cos(ang)
+            R[a, b], R[b, a] = -np.sin(ang), np.sin(ang)
+            G = G @ R
+        return e, G[:, :n].copy()
+
+    class _Synthetic(DelvesHamiltonian):
+        def __post_init__(self):
+            pass
+
+        def surface(self, rho):
+            e, C = surface_at(rho)
+            return DelvesSurface(rho=rho, energies=e, coefficients=C, overlap_eigenvalues=np.ones(e.size))
+
+        def transform(self, a, b):
+            return a.coefficients.T @ b.coefficients
+
+    ham = _Synthetic(basis=_Basis(), total_potential=None)
+    sectors = build_radial_sectors((2.0, 6.0), (0.05,))
+    energies = np.array([0.035, 0.05, 0.08])
+    rho = np.array([s.radial_mid for s in sectors])
+    E_s = np.zeros((rho.size, 5))
+    C_s = np.zeros((rho.size, n_primitive, 5))
+    n_s = np.zeros(rho.size, dtype=np.int64)
+    for i, r in enumerate(rho):
+        e, C = surface_at(r)
+        n_s[i] = e.size
+        E_s[i, : e.size] = e
+        C_s[i, :, : e.size] = C
+    out = {}
+    for mode in ("inelastic", "capture"):
+        res = ref_propagate_delves(ham, energies, sectors, ticc.Propagation(mode=mode))
+        out[f"Y_{mode}"] = np.asarray(res.Y_final)
+    _save("delves", {"rho_min": 2.0, "rho_max": 6.0, "half_step": 0.05, "masses_amu": [1.0, 2.0, 19.0]},
+          energies=energies, rho=rho, surface_energies=E_s, surface_coefficients=C_s, n_surface=n_s, **out)
+
 MAKERS = {
     "ldmd": make_ldmd,
     "contract": make_contract,
@@ -769,6 +827,7 @@ MAKERS = {
     "dropin": make_dropin,
     "contract_families": make_contract_families,
     "contract_fs": make_contract_fs,
+    "delves": make_delves,
 }
 # benchmark-size fixtures: run by name only (tens of minutes of CPU in total);
 # ``full_morse`` takes optional parities after its name: ``make_golden.py <src> full_morse -1``
