@@ -3,6 +3,7 @@
 // Each entry validates its arguments on the host, carves the caller's workspace into
 // 256-byte aligned regions, enqueues the kernels on the caller's stream and returns a
 // status code; the message of the last failure is kept per host thread.
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -284,14 +285,32 @@ int ticc_contract(const double* rows_real, const double* rows_imag, const int* g
   ticc::contract_init_kernel<<<ticc::grid_for((long long)n_R * n_channel * n_channel, 256), 256, 0, s>>>(out, n_channel, n_R, radial_points, U, E_int, reduced_mass);
   ticc::note_launch();
   const double scale = normalization * (U != nullptr ? 2.0 * reduced_mass : 1.0);
+  cudaError_t e = cudaFuncSetAttribute(ticc::contract_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ticc::kVSmemBytes);
+  if (e != cudaSuccess) return cuda_fail(e, "ticc_contract");
+  // one launch per kVMaxGroups non-empty groups (and per 65535 radial points)
+  ticc::ContractTiles tiles{};
+  auto flush = [&]() {
+    const int n_tiles = tiles.tile_start[tiles.n_groups];
+    for (int r0 = 0; r0 < n_R; r0 += 65535) {
+      ticc::contract_group_kernel<<<dim3(n_tiles, std::min(65535, n_R - r0)), 256, ticc::kVSmemBytes, s>>>(tiles, rows_real, rows_imag, row_out, n_grid, scale, potential,
+                                                                                                     pot_stride, r0, n_channel, out);
+      ticc::note_launch();
+    }
+    tiles.n_groups = 0;
+    tiles.tile_start[0] = 0;
+  };
   for (int g = 0; g < n_groups; ++g) {
     const int rows = group_offsets[g + 1] - group_offsets[g];
     if (rows == 0) continue;
-    const int t = (rows + ticc::kCTile - 1) / ticc::kCTile;
-    ticc::contract_group_kernel<<<dim3(t * (t + 1) / 2, n_R), 256, 0, s>>>(rows_real, rows_imag, group_offsets[g], rows, row_out, n_grid, scale, potential, pot_stride, n_channel, out);
-    ticc::note_launch();
+    const int t = (rows + ticc::kVTile - 1) / ticc::kVTile;
+    const int k = tiles.n_groups++;
+    tiles.row0[k] = group_offsets[g];
+    tiles.rows[k] = rows;
+    tiles.tile_start[k + 1] = tiles.tile_start[k] + t * (t + 1) / 2;
+    if (tiles.n_groups == ticc::kVMaxGroups) flush();
   }
-  cudaError_t e = cudaGetLastError();
+  if (tiles.n_groups > 0) flush();
+  e = cudaGetLastError();
   return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_contract");
 }
 
@@ -304,10 +323,14 @@ int ticc_contract_block(const double* A, int n_a, const double* B, int n_b, int 
     return fail(TICC_ERR_INVALID_ARGUMENT, "ticc_contract_block: n_a=%d n_b=%d n_grid=%d n_R=%d n=%d w_stride=%lld symmetric=%d (a symmetric block has B = A)", n_a, n_b,
                 n_grid, n_R, n, w_stride, symmetric);
   if (n_a == 0 || n_b == 0 || n_R == 0) return TICC_OK;
-  const dim3 grid((n_a + ticc::kCTile - 1) / ticc::kCTile, (n_b + ticc::kCTile - 1) / ticc::kCTile, n_R);
-  ticc::weighted_block_kernel<<<grid, 256, 0, as_stream(stream)>>>(A, n_a, B, n_b, n_grid, weights, w_stride, pos_a, pos_b, symmetric, mirror, n, out);
-  ticc::note_launch();
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = cudaFuncSetAttribute(ticc::weighted_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ticc::kVSmemBytes);
+  if (e != cudaSuccess) return cuda_fail(e, "ticc_contract_block");
+  for (int r0 = 0; r0 < n_R; r0 += 65535) {
+    const dim3 grid((n_a + ticc::kVTile - 1) / ticc::kVTile, (n_b + ticc::kVTile - 1) / ticc::kVTile, std::min(65535, n_R - r0));
+    ticc::weighted_block_kernel<<<grid, 256, ticc::kVSmemBytes, as_stream(stream)>>>(A, n_a, B, n_b, n_grid, weights, w_stride, r0, pos_a, pos_b, symmetric, mirror, n, out);
+    ticc::note_launch();
+  }
+  e = cudaGetLastError();
   return e == cudaSuccess ? TICC_OK : cuda_fail(e, "ticc_contract_block");
 }
 

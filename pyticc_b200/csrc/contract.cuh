@@ -2,17 +2,17 @@
 //
 // For one K group with weighted rows B (n_K x n_grid) and PES values v(R) on the
 // quadrature grid, V_K(R)[a][b] = norm sum_q (Br[a][q] Br[b][q] + Bi[a][q] Bi[b][q]) v[q].
-// Each CTA computes a 32x32 lower-triangular tile of one group at one R and writes both
-// (a, b) and (b, a), so V is exactly symmetric (the reference symmetrises explicitly).
-// The init kernel writes U/R^2 + 2 mu diag(E_int) (or zeros when only V is wanted) and
-// the group kernels add 2 mu V (or V) at the rows' output channel positions.
+// One launch covers every group: each CTA computes a 64x64 lower-triangular tile of one group
+// at one R on the FP64 tensor pipe and writes both (a, b) and (b, a), so V is exactly symmetric
+// (the reference symmetrises explicitly).  The init kernel writes U/R^2 + 2 mu diag(E_int) (or
+// zeros when only V is wanted) and the group kernel adds 2 mu V (or V) at the rows' output
+// channel positions.
 #pragma once
 
+#include "dmma_tile.cuh"
 #include "ticc_common.cuh"
 
 namespace ticc {
-
-constexpr int kCTile = 32;
 
 __global__ void contract_init_kernel(double* out, int n, int n_R, const double* radial_points, const double* U, const double* E_int, double mu) {
   const long long total = (long long)n_R * n * n;
@@ -30,117 +30,167 @@ __global__ void contract_init_kernel(double* out, int n, int n_R, const double* 
   }
 }
 
-// grid: (lower tile pairs of the group, n_R); block 16 x 16 threads, 2 x 2 outputs each.
-__global__ void __launch_bounds__(256) contract_group_kernel(const double* __restrict__ Br, const double* __restrict__ Bi, int row0, int n_rows, const int* __restrict__ row_out, int n_grid, double scale, const double* __restrict__ potential, long long pot_stride, int n, double* __restrict__ out) {
-  __shared__ double As[kCTile][kCTile + 1];
-  __shared__ double Bs[kCTile][kCTile + 1];
-  __shared__ double Ai[kCTile][kCTile + 1];
-  __shared__ double Bj[kCTile][kCTile + 1];
-  __shared__ double vs[kCTile];
-  int ta = (int)((sqrt(8.0 * blockIdx.x + 1.0) - 1.0) * 0.5);
-  while ((ta + 1) * (ta + 2) / 2 <= (int)blockIdx.x) ++ta;
-  while (ta * (ta + 1) / 2 > (int)blockIdx.x) --ta;
-  const int tb = blockIdx.x - ta * (ta + 1) / 2;
-  const int r = blockIdx.y;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const double* v = potential + (long long)r * pot_stride;
-  const bool imag = (Bi != nullptr);
-  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
-  for (int q0 = 0; q0 < n_grid; q0 += kCTile) {
-    for (int idx = threadIdx.x; idx < kCTile * kCTile; idx += 256) {
-      const int rr = idx / kCTile, qq = idx % kCTile;
-      const int q = q0 + qq;
-      const int ra = ta * kCTile + rr, rb = tb * kCTile + rr;
-      const bool qin = q < n_grid;
-      As[qq][rr] = (qin && ra < n_rows) ? Br[(long long)(row0 + ra) * n_grid + q] : 0.0;
-      Bs[qq][rr] = (qin && rb < n_rows) ? Br[(long long)(row0 + rb) * n_grid + q] : 0.0;
-      if (imag) {
-        Ai[qq][rr] = (qin && ra < n_rows) ? Bi[(long long)(row0 + ra) * n_grid + q] : 0.0;
-        Bj[qq][rr] = (qin && rb < n_rows) ? Bi[(long long)(row0 + rb) * n_grid + q] : 0.0;
-      }
+// ---- the weighted-product tile on the FP64 tensor pipe ------------------------------------------
+// A CTA of 8 warps computes one 64 x 64 tile X[i][j] = sum_q A[i][q] w[q] B[j][q] (plus the same
+// over a second pair A2, B2: the imaginary rows of a complex basis) with mma.sync m8n8k4 f64
+// (DMMA), FP64 accumulation.  The rows are read as stored (row-major, q contiguous, any n_grid
+// and any row offset) in chunks of 32 grid points: each warp loads whole 256-byte row segments,
+// the weight is applied to A on the way into shared memory, and rows past the operand's end read
+// as zeros.  Shared tiles are [row][q] with a row stride of 36 doubles, so the fragment loads of a
+// half-warp (rows mr = 0..3, k = 0..3) hit 16 distinct bank pairs.  Chunk c + 1 is fetched into
+// registers while chunk c is multiplied from the other shared buffer (one barrier per chunk).
+// Warp w owns rows (w / 4) * 32 .. +31 and columns (w % 4) * 16 .. +15 of the tile: 4 x 2 DMMA
+// accumulators, element [mt][nt][h] at row (w/4)*32 + 8 mt + lane/4, column (w%4)*16 + 8 nt +
+// 2 (lane%4) + h.
+constexpr int kVTile = 64;
+constexpr int kVChunk = 32;
+constexpr int kVLd = kVChunk + 4;
+constexpr int kVMaxGroups = 128;
+constexpr size_t kVSmemBytes = size_t(2) * 2 * kVTile * kVLd * sizeof(double);  // 73728
+
+struct VTileAcc {
+  double v[4][2][2];
+};
+
+// A, B (and A2, B2) point at the tile's first row; rows at or beyond na (nb) read as zero.
+__device__ inline void vtile_product(VTileAcc& acc, const double* __restrict__ A, int na, const double* __restrict__ B, int nb, const double* __restrict__ A2,
+                                     const double* __restrict__ B2, int n_grid, const double* __restrict__ w, double* smem) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int qq = lane, rbase = warp;  // loader: grid point q0 + lane of rows warp + 8 i
+  const int wm = (warp >> 2) * 32, wn = (warp & 3) * 16, kr = lane & 3, mr = lane >> 2;
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) acc.v[mt][nt][0] = acc.v[mt][nt][1] = 0.0;
+  const int nq = (n_grid + kVChunk - 1) / kVChunk;
+  const int nc = A2 != nullptr ? 2 * nq : nq;
+  double ra[8], rb[8];
+  auto fetch = [&](int c) {
+    const bool second = c >= nq;
+    const double* sa = second ? A2 : A;
+    const double* sb = second ? B2 : B;
+    const int q = (second ? c - nq : c) * kVChunk + qq;
+    const bool in = q < n_grid;
+    const double wq = in ? w[q] : 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int row = rbase + 8 * i;
+      ra[i] = (in && row < na) ? sa[(long long)row * n_grid + q] * wq : 0.0;
+      rb[i] = (in && row < nb) ? sb[(long long)row * n_grid + q] : 0.0;
     }
-    if (threadIdx.x < kCTile) vs[threadIdx.x] = (q0 + threadIdx.x < n_grid) ? v[q0 + threadIdx.x] : 0.0;
-    __syncthreads();
-#pragma unroll 8
-    for (int qq = 0; qq < kCTile; ++qq) {
-      const double w = vs[qq];
-      const double a0 = As[qq][ty] * w, a1 = As[qq][ty + 16] * w;
-      const double b0 = Bs[qq][tx], b1 = Bs[qq][tx + 16];
-      acc[0][0] += a0 * b0;
-      acc[0][1] += a0 * b1;
-      acc[1][0] += a1 * b0;
-      acc[1][1] += a1 * b1;
-      if (imag) {
-        const double c0 = Ai[qq][ty] * w, c1 = Ai[qq][ty + 16] * w;
-        const double d0 = Bj[qq][tx], d1 = Bj[qq][tx + 16];
-        acc[0][0] += c0 * d0;
-        acc[0][1] += c0 * d1;
-        acc[1][0] += c1 * d0;
-        acc[1][1] += c1 * d1;
-      }
+  };
+  auto put = [&](double* buf) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      buf[(rbase + 8 * i) * kVLd + qq] = ra[i];
+      buf[kVTile * kVLd + (rbase + 8 * i) * kVLd + qq] = rb[i];
     }
+  };
+  fetch(0);
+  put(smem);
+  __syncthreads();
+  for (int c = 0; c < nc; ++c) {
+    if (c + 1 < nc) fetch(c + 1);
+    const double* As = smem + (c & 1) * 2 * kVTile * kVLd;
+    const double* Bs = As + kVTile * kVLd;
+#pragma unroll
+    for (int kk = 0; kk < kVChunk; kk += 4) {
+      double a[4], b[2];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt) a[mt] = As[(wm + mt * 8 + mr) * kVLd + kk + kr];
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) b[nt] = Bs[(wn + nt * 8 + mr) * kVLd + kk + kr];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) dmma_8x8x4(acc.v[mt][nt], a[mt], b[nt]);
+    }
+    if (c + 1 < nc) put(smem + ((c + 1) & 1) * 2 * kVTile * kVLd);
     __syncthreads();
   }
+}
+
+// Lower 64-tiles of every K group in one launch: tile t belongs to the group g with
+// tile_start[g] <= t < tile_start[g + 1] (only groups with rows are listed).
+struct ContractTiles {
+  int n_groups;
+  int tile_start[kVMaxGroups + 1];
+  int row0[kVMaxGroups];
+  int rows[kVMaxGroups];
+};
+
+// grid: (the table's tiles, radial points r_first ..); 256 threads; kVSmemBytes dynamic shared memory.
+__global__ void __launch_bounds__(256) contract_group_kernel(const __grid_constant__ ContractTiles tiles, const double* __restrict__ Br, const double* __restrict__ Bi,
+                                                             const int* __restrict__ row_out, int n_grid, double scale, const double* __restrict__ potential,
+                                                             long long pot_stride, int r_first, int n, double* __restrict__ out) {
+  extern __shared__ __align__(16) double vsmem[];
+  const int t = blockIdx.x;
+  int g = 0, hi = tiles.n_groups - 1;
+  while (g < hi) {  // the last group whose first tile is at or before t
+    const int mid = (g + hi + 1) >> 1;
+    if (tiles.tile_start[mid] <= t) g = mid;
+    else hi = mid - 1;
+  }
+  const int local = t - tiles.tile_start[g];
+  int ta = (int)((sqrt(8.0 * local + 1.0) - 1.0) * 0.5);
+  while ((ta + 1) * (ta + 2) / 2 <= local) ++ta;
+  while (ta * (ta + 1) / 2 > local) --ta;
+  const int tb = local - ta * (ta + 1) / 2;
+  const int row0 = tiles.row0[g], rows = tiles.rows[g];
+  const int r = r_first + blockIdx.y;
+  const long long ia = (long long)(row0 + ta * kVTile) * n_grid, ib = (long long)(row0 + tb * kVTile) * n_grid;
+  VTileAcc acc;
+  vtile_product(acc, Br + ia, rows - ta * kVTile, Br + ib, rows - tb * kVTile, Bi != nullptr ? Bi + ia : nullptr, Bi != nullptr ? Bi + ib : nullptr, n_grid,
+                potential + (long long)r * pot_stride, vsmem);
   double* o = out + (long long)r * n * n;
-  for (int u = 0; u < 2; ++u)
-    for (int w = 0; w < 2; ++w) {
-      const int a = ta * kCTile + ty + 16 * u;
-      const int b = tb * kCTile + tx + 16 * w;
-      if (a >= n_rows || b >= n_rows || b > a) continue;
-      const int pa = row_out[row0 + a], pb = row_out[row0 + b];
-      const double val = scale * acc[u][w];
-      o[(long long)pa * n + pb] += val;
-      if (a != b) o[(long long)pb * n + pa] += val;
-    }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = (warp >> 2) * 32, wn = (warp & 3) * 16;
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int a = ta * kVTile + wm + mt * 8 + (lane >> 2);
+        const int b = tb * kVTile + wn + nt * 8 + 2 * (lane & 3) + h;
+        if (a >= rows || b >= rows || b > a) continue;
+        const int pa = row_out[row0 + a], pb = row_out[row0 + b];
+        const double val = scale * acc.v[mt][nt][h];
+        o[(long long)pa * n + pb] += val;
+        if (a != b) o[(long long)pb * n + pa] += val;
+      }
 }
 
 // One block of a state-resolved (diabatic) contraction at every R:
 //     X(R)[i][j] = sum_q A[i][q] w(R)[q] B[j][q],   A: n_a x n_grid, B: n_b x n_grid (row strides n_grid)
 // written to out(R)[pos_a[i]][pos_b[j]] and, with `mirror`, also to out(R)[pos_b[j]][pos_a[i]].
 // A symmetric block (`symmetric`: B is A and pos_b is pos_a) computes only i >= j and writes
-// both (i, j) and (j, i), so the block is exactly symmetric.  grid: (tiles of A, tiles of B,
-// n_R); block 16 x 16 threads, 2 x 2 outputs each.
+// both (i, j) and (j, i), so the block is exactly symmetric.  grid: (64-tiles of A, 64-tiles of B,
+// radial points r_first ..); 256 threads; kVSmemBytes dynamic shared memory.
 __global__ void __launch_bounds__(256) weighted_block_kernel(const double* __restrict__ A, int n_a, const double* __restrict__ B, int n_b, int n_grid, const double* __restrict__ w,
-                                                             long long w_stride, const int* __restrict__ pos_a, const int* __restrict__ pos_b, int symmetric, int mirror, int n,
-                                                             double* __restrict__ out) {
-  const int ti = blockIdx.x, tj = blockIdx.y, R = blockIdx.z;
+                                                             long long w_stride, int r_first, const int* __restrict__ pos_a, const int* __restrict__ pos_b, int symmetric,
+                                                             int mirror, int n, double* __restrict__ out) {
+  extern __shared__ __align__(16) double vsmem[];
+  const int ti = blockIdx.x, tj = blockIdx.y, R = r_first + blockIdx.z;
   if (symmetric && tj > ti) return;
-  __shared__ double As[kCTile][kCTile + 1];
-  __shared__ double Bs[kCTile][kCTile + 1];
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int i0 = ti * kCTile, j0 = tj * kCTile;
-  const double* wr = w + (long long)R * w_stride;
-  double acc[2][2] = {};
-  for (int q0 = 0; q0 < n_grid; q0 += kCTile) {
-    for (int e = threadIdx.x; e < kCTile * kCTile; e += 256) {
-      const int rr = e / kCTile, qq = e % kCTile, q = q0 + qq;
-      const bool inq = q < n_grid;
-      As[rr][qq] = (inq && i0 + rr < n_a) ? A[(long long)(i0 + rr) * n_grid + q] * wr[q] : 0.0;
-      Bs[rr][qq] = (inq && j0 + rr < n_b) ? B[(long long)(j0 + rr) * n_grid + q] : 0.0;
-    }
-    __syncthreads();
-#pragma unroll 8
-    for (int qq = 0; qq < kCTile; ++qq) {
-      const double a0 = As[ty][qq], a1 = As[ty + 16][qq];
-      const double b0 = Bs[tx][qq], b1 = Bs[tx + 16][qq];
-      acc[0][0] = fma(a0, b0, acc[0][0]);
-      acc[0][1] = fma(a0, b1, acc[0][1]);
-      acc[1][0] = fma(a1, b0, acc[1][0]);
-      acc[1][1] = fma(a1, b1, acc[1][1]);
-    }
-    __syncthreads();
-  }
+  const int i0 = ti * kVTile, j0 = tj * kVTile;
+  VTileAcc acc;
+  vtile_product(acc, A + (long long)i0 * n_grid, n_a - i0, B + (long long)j0 * n_grid, n_b - j0, nullptr, nullptr, n_grid, w + (long long)R * w_stride, vsmem);
   double* o = out + (long long)R * n * n;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = (warp >> 2) * 32, wn = (warp & 3) * 16;
 #pragma unroll
-  for (int u = 0; u < 2; ++u)
+  for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
-    for (int v = 0; v < 2; ++v) {
-      const int i = i0 + ty + 16 * u, j = j0 + tx + 16 * v;
-      if (i >= n_a || j >= n_b || (symmetric && j > i)) continue;
-      const int pa = pos_a[i], pb = pos_b[j];
-      o[(long long)pa * n + pb] = acc[u][v];
-      if (mirror || (symmetric && i != j)) o[(long long)pb * n + pa] = acc[u][v];
-    }
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int i = i0 + wm + mt * 8 + (lane >> 2), j = j0 + wn + nt * 8 + 2 * (lane & 3) + h;
+        if (i >= n_a || j >= n_b || (symmetric && j > i)) continue;
+        const int pa = pos_a[i], pb = pos_b[j];
+        o[(long long)pa * n + pb] = acc.v[mt][nt][h];
+        if (mirror || (symmetric && i != j)) o[(long long)pb * n + pa] = acc.v[mt][nt][h];
+      }
 }
 
 

@@ -140,6 +140,39 @@ def ultracold_capture(*, B_cm=0.03, jmax=40, J=10, parity=1, mu_amu=100.0, C6=1.
     return Workload("ultracold_capture", system, prepare_potential(system, boundaries, half_steps, n_theta=n_theta), energies, mode="capture")
 
 
+def _time_contraction(system: str, n_points: int, repeat: int) -> None:
+    """Best-of-``repeat`` time of one ``ticc_contract`` call over ``n_points`` radial points of the
+    vibrating A+BC system (N = 1984, 1024 grid points, real rows) or the AB+CD rotor pair (N = 2610,
+    2700 grid points, complex rows); the rate counts the lower-triangle multiply-adds of every K
+    group, 2 n_grid (x2 for complex rows) flops per channel pair."""
+    import torch
+
+    from .matrix.interaction import contract_rows, device_rows
+    from .scattering import build_hamiltonian
+
+    wl = morse_atom_diatom() if system == "morse" else rotor_pair()
+    vb = build_hamiltonian(wl.system, wl.grid).V_basis
+    dev = torch.device("cuda", 0)
+    rows = device_rows(vb, dev)
+    points = wl.grid.radial_points[np.linspace(0, wl.grid.radial_points.size - 1, n_points).astype(int)]
+    values = wl.grid.take_device(points, dev).reshape(n_points, -1).contiguous()
+    out = contract_rows(rows, values)
+    torch.cuda.synchronize()
+    best = None
+    for _ in range(repeat):
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        contract_rows(rows, values, out=out)
+        end.record()
+        torch.cuda.synchronize()
+        best = start.elapsed_time(end) if best is None else min(best, start.elapsed_time(end))
+    parts = 2 if vb.B_imag is not None else 1
+    pairs = sum(len(m) * (len(m) + 1) // 2 for m in vb.channel_indices.values())
+    flops = 2.0 * rows.n_grid * parts * pairs * n_points
+    print(f"contract {system}: N={vb.n_channel} n_grid={rows.n_grid} parts={parts} points={n_points}: {best:.3f} ms ({best / n_points * 1e3:.1f} us/point), "
+          f"{flops / (best * 1e-3) / 1e12:.2f} TF/s FP64 (lower-triangle work)")
+
+
 def _propagate_window(argv=None) -> None:
     """Propagate a window of the bench system's sectors once (a small, fixed case for
     profilers): ``python -m pyticc_b200.workloads --precision mixed --first 100 --sectors 8``."""
@@ -157,7 +190,12 @@ def _propagate_window(argv=None) -> None:
     p.add_argument("--sectors", type=int, default=8)
     p.add_argument("--energies", type=int, default=16, help="every 256/energies-th of the bench energies")
     p.add_argument("--repeat", type=int, default=0, help="also time the LDMD launches this many times (CUDA events) and print the best ms per sector")
+    p.add_argument("--contract", choices=["morse", "pair"], default=None, help="time the V(R) contraction of this system instead (CUDA events, --points radial points per call)")
+    p.add_argument("--points", type=int, default=64, help="radial points per contraction call")
     args = p.parse_args(argv)
+    if args.contract is not None:
+        _time_contraction(args.contract, args.points, max(args.repeat, 1))
+        return
     wl = morse_atom_diatom()
     ham = hamiltonian_for(wl.system, wl.grid)
     energies = wl.energies[:: max(1, wl.energies.size // args.energies)][: args.energies]
