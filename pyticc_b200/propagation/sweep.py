@@ -208,7 +208,7 @@ class PartialWaveSweep:
         skipped = sum(1 for n in self.sizes if n == 0)
         if skipped:
             logger.info(f"Partial-wave sweep: {skipped} block(s) without channels skipped")
-        closed_first = propagation.precision == "mixed"
+        closed_first = True  # the propagation order at every precision (runner.DeviceHamiltonian)
         self.states = {}
         for i, system in enumerate(self.systems):
             if self.sizes[i]:

@@ -173,6 +173,35 @@ def _time_contraction(system: str, n_points: int, repeat: int) -> None:
           f"{flops / (best * 1e-3) / 1e12:.2f} TF/s FP64 (lower-triangle work)")
 
 
+def _time_pair_solve(n_energy: int) -> None:
+    """Wall time of one ``solve`` of the AB+CD rotor pair (N = 2610, 275 sectors) over every
+    128/n_energy-th of its 128 energies, plain FP64 then mixed precision, after a one-energy
+    warm-up solve that builds the Hamiltonian and its device caches."""
+    from time import perf_counter
+
+    import torch
+
+    from .propagation.config import Propagation
+    from .scattering import solve
+
+    wl = rotor_pair()
+    energies = wl.energies[:: max(1, wl.energies.size // n_energy)][:n_energy]
+    solve(wl.system, energies[:1], wl.grid, Propagation(precision="fp64"))
+    results = {}
+    for precision in ("fp64", "mixed"):
+        stats: dict = {}
+        torch.cuda.synchronize()
+        started = perf_counter()
+        result = solve(wl.system, energies, wl.grid, Propagation(precision=precision), stats=stats)
+        torch.cuda.synchronize()
+        wall = perf_counter() - started
+        results[precision] = result
+        print(f"pair N={wl.system.basis.n_channel} sectors={len(wl.grid.sectors)} {precision}: {energies.size} energies in {wall:.2f} s = {energies.size / wall:.2f} solves/s, "
+              f"reduced sweep steps {stats.get('reduced_steps', 0)} of {stats.get('sweep_steps', 0)}, unitarity defect {result.unitarity_defect().max():.1e}")
+    dS = max((float(np.abs(a - b).max()) for a, b in zip(results["fp64"].Smat, results["mixed"].Smat) if a.size), default=0.0)
+    print(f"pair mixed vs fp64 max|dS| {dS:.2e}")
+
+
 def _propagate_window(argv=None) -> None:
     """Propagate a window of the bench system's sectors once (a small, fixed case for
     profilers): ``python -m pyticc_b200.workloads --precision mixed --first 100 --sectors 8``."""
@@ -192,9 +221,13 @@ def _propagate_window(argv=None) -> None:
     p.add_argument("--repeat", type=int, default=0, help="also time the LDMD launches this many times (CUDA events) and print the best ms per sector")
     p.add_argument("--contract", choices=["morse", "pair"], default=None, help="time the V(R) contraction of this system instead (CUDA events, --points radial points per call)")
     p.add_argument("--points", type=int, default=64, help="radial points per contraction call")
+    p.add_argument("--solve-pair", action="store_true", help="time whole solves of the AB+CD rotor pair (N = 2610) for --energies energies, FP64 and mixed")
     args = p.parse_args(argv)
     if args.contract is not None:
         _time_contraction(args.contract, args.points, max(args.repeat, 1))
+        return
+    if args.solve_pair:
+        _time_pair_solve(args.energies)
         return
     wl = morse_atom_diatom()
     ham = hamiltonian_for(wl.system, wl.grid)

@@ -342,8 +342,9 @@ def make_solve_morse() -> None:
     np.savez_compressed(HERE / "morse_rovib.npz", grids=rovib.grids, E_vj=rovib.E_vj, WF_vj=rovib.WF_vj)
 
 
-def make_solve_diatom_diatom() -> None:
-    params = {"B1_cm": 60.0, "B2_cm": 2.0, "jmax": 2, "J": 1, "mu_amu": 3.6, "lmax": 2, "seed": 11, "strength_cm": 40.0, "lj_eps_cm": 100.0, "lj_Rm": 6.0, "n_theta_X": 6, "n_theta_Y": 6, "n_phi": 5, "boundaries": [4.0, 10.0], "half_steps": [0.05]}
+def _bispherical_pes(params):
+    """sum_(l1,l2,l) c strength exp(-0.8 (R-6)) A_{l1 l2 l} + LJ, c ~ N(0,1) seeded, with the
+    reference's own angular functions."""
     from pyticc.basis.angle import clebsch_gordan, norm_YjK
 
     rng = np.random.default_rng(params["seed"])
@@ -367,6 +368,12 @@ def make_solve_diatom_diatom() -> None:
         lj = params["lj_eps_cm"] * CM * ((params["lj_Rm"] / R) ** 12 - 2.0 * (params["lj_Rm"] / R) ** 6)
         return radial * total + lj
 
+    return terms, interaction
+
+
+def make_solve_diatom_diatom() -> None:
+    params = {"B1_cm": 60.0, "B2_cm": 2.0, "jmax": 2, "J": 1, "mu_amu": 3.6, "lmax": 2, "seed": 11, "strength_cm": 40.0, "lj_eps_cm": 100.0, "lj_Rm": 6.0, "n_theta_X": 6, "n_theta_Y": 6, "n_phi": 5, "boundaries": [4.0, 10.0], "half_steps": [0.05]}
+    terms, interaction = _bispherical_pes(params)
     params["terms"] = terms
     diatom_X = _rigid_rotor(params["B1_cm"], params["jmax"])
     diatom_Y = _rigid_rotor(params["B2_cm"], params["jmax"])
@@ -604,6 +611,21 @@ def make_full_morse() -> None:
         _solve_full_and_save(f"full_morse_J30_p{tag}", {**params, "parity": parity}, system, params["boundaries"], params["half_steps"], energies, "inelastic", n_theta=params["n_theta"])
 
 
+def make_full_pair() -> None:
+    """The AB+CD rigid-rotor pair at full size: j1, j2 <= 8, J = 6, parity +1, no channel or
+    energy cutoff (N = 2610), 275 sectors, three energies of its 5-800 cm^-1 grid (5, 105.2 and
+    555.9 cm^-1; 3, 28 and 345 open channels)."""
+    params = {"B1_cm": 60.0, "B2_cm": 2.0, "jmax": 8, "J": 6, "parity": 1, "mu_amu": 3.6, "lmax": 4, "seed": 11, "strength_cm": 40.0, "lj_eps_cm": 100.0, "lj_Rm": 6.0,
+              "n_theta_X": 15, "n_theta_Y": 15, "n_phi": 12, "boundaries": [2.5, 30.0], "half_steps": [0.05], "energy_indices": [0, 16, 88]}
+    terms, interaction = _bispherical_pes(params)
+    params["terms"] = terms
+    energies = np.linspace(5.0, 800.0, 128)[params["energy_indices"]] * CM
+    system = ticc.build_ScattSystem(_rigid_rotor(params["B1_cm"], params["jmax"]), _rigid_rotor(params["B2_cm"], params["jmax"]), Jtot=params["J"], system_parity=1,
+                                    potential=ticc.PESWrapper(interaction=interaction), reduced_mass=params["mu_amu"] * AMU)
+    _solve_full_and_save("full_pair_J6", params, system, params["boundaries"], params["half_steps"], energies, "inelastic", n_theta_X=params["n_theta_X"],
+                         n_theta_Y=params["n_theta_Y"], n_phi=params["n_phi"])
+
+
 def make_full_capture() -> None:
     """The ultracold capture block at full size: rigid rotor B=0.03 cm^-1, j<=40, J=10 (N=396;
     optional other J values after the name: ``make_golden.py <src> full_capture 0 1``),
@@ -835,6 +857,7 @@ FULL_SIZE_MAKERS = {
     "full_rigid": make_full_rigid,
     "full_morse": make_full_morse,
     "full_capture": make_full_capture,
+    "full_pair": make_full_pair,
 }
 
 if __name__ == "__main__":
