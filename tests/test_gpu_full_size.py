@@ -156,9 +156,8 @@ def test_pair_full_size_fp64_matches_reference(pair):
 
     At 5 and 105 cm^-1 FP64 holds 1e-8.  At 556 cm^-1 (345 open channels) the reference's LU
     pivots over the whole matrix while the sweep pivots inside 64-wide sub-blocks: in the
-    closed-first order a CPU emulation of the sweep loses 3.7e-8 there and the device's
-    mixed-precision run of that order 2.3e-7 (the basis order lost 6e-3 on the device), so
-    that energy is held to PAIR_HIGH_TOL."""
+    closed-first order a CPU emulation of the sweep loses 3.7e-8 there and the device 2.4e-7
+    (the basis order lost 6e-3 on the device), so that energy is held to PAIR_HIGH_TOL."""
     wl, data = pair
     result, _ = _solve(wl, data)
     dS = _dS_per_energy(result, data)
